@@ -1,0 +1,315 @@
+"""Benchmark of the batched ComplexF32 transform hot path on B200.
+
+Workload: batched ComplexF32 forward FFTs of length N=4096, 16384 columns per
+GPU (the target configuration named for FFTA's batched path; configuration 2
+shapes, inputs i.i.d. complex normal from a seed).  One step is one forward
+transform of the whole batch.  Inputs (512 MiB) and outputs (512 MiB) are each
+larger than the 126 MB L2, so no flush is needed between steps.
+
+  value     GFLOP/s (5 N log2 N per transform) over all ranks, inputs resident in HBM
+  e2e       the same metric through the C ABI's host-array entry point
+            (fb_execute_host) from pinned host memory: H2D + transform + D2H
+  roofline  achieved HBM GB/s of the line kernel (2 N B sizeof(C) algorithmic
+            bytes per launch / CUDA-event launch time) against the measured
+            copy bandwidth in MEASURED_PEAKS.json
+  cpu_baseline  the oracle (C++ restatement of FFTA's algorithm) on the host's
+            cores over a bounded sample of the same workload
+
+`--impl reference` times FFTA's algorithm on the host cores (the oracle, as
+FFTA itself -- Julia -- is not installed) on the same metric.
+Multi-GPU: one process per GPU (torchrun), each transforming its own 16384
+columns (weak scaling, no collective on the data path); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ffta.jl_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+N = 4096
+BATCH = 16384
+ES = 8  # bytes per ComplexF32
+EXTRA = [(19683, 2 ** 24 // 19683), (27648, 2 ** 24 // 27648), (2 ** 20, 16)]
+
+
+def flops(n, b):
+    return 5.0 * n * np.log2(n) * b
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def cpu_baseline(n, sample_cols, nthreads, direction=-1):
+    """Time the oracle (FFTA's algorithm restated in C++) on host cores."""
+    import oracle
+    rng = np.random.default_rng(7)
+    x = (rng.standard_normal((sample_cols, n)) + 1j * rng.standard_normal((sample_cols, n))
+         ).astype(np.complex64)
+    oracle.fft_batched(x[:min(8, sample_cols)], direction, nthreads=1)  # warm
+    t0 = time.perf_counter()
+    oracle.fft_batched(x, direction, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    return flops(n, sample_cols) / dt / 1e9, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    nthreads = os.cpu_count() or 1
+    sample = 1024  # columns per step: a bounded sample of the 16384-column batch
+    for _ in range(args.warmup):
+        cpu_baseline(N, sample, nthreads)
+    times = []
+    for _ in range(args.steps):
+        _, dt = cpu_baseline(N, sample, nthreads)
+        times.append(dt)
+    tot = float(np.sum(times))
+    value = flops(N, sample) * args.steps / tot / 1e9
+    line = {
+        "impl": "reference", "metric": "batched FFT GFLOP/s (5 N log2 N), C32 N=4096",
+        "value": value, "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"batched C32 forward FFT N={N}, {sample}-column sample per "
+                               f"step of the {BATCH}-column batch", "n": N, "batch": sample},
+        "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": nthreads, "kind": "port",
+                         "sample": f"{sample} transforms of N={N} per step, batch split over "
+                                   f"{nthreads} threads (FFTA itself is single-threaded)"},
+        "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "FFTA.jl (Julia) is not installed on this image; the reference arm runs the "
+                "C++ restatement of FFTA's algorithm (oracle/ffta_oracle.cpp)",
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-extra", action="store_true", help="skip the other batched sizes")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    args.warmup = max(args.warmup, 3)
+
+    import torch
+    import torch.distributed as dist
+    import ffta_b200 as F
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    g = torch.Generator(device=dev)
+    g.manual_seed(1234 + rank)
+    # Julia N x B column-major matrix = torch (B, N) row-major; columns contiguous
+    x = torch.complex(torch.randn(BATCH, N, device=dev, generator=g),
+                      torch.randn(BATCH, N, device=dev, generator=g))
+    y = torch.empty_like(x)
+    p = F.plan_fft(x.T, 1)
+    xt, yt = x.T, y.T
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        F.mul_(yt, p, xt)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    launches_per_step = p.describe(xt).count("(")  # one line-kernel launch per pass
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms_max = max_over_ranks(ms)
+    total_flops = flops(N, BATCH) * world
+    value = total_flops / (ms_max * 1e-3) / 1e9
+    alg_bytes = 2.0 * N * BATCH * ES
+    achieved = alg_bytes / (ms * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+
+    # accuracy spot check of this run against the FP64 oracle on a few columns
+    import oracle
+    cols = [0, BATCH // 2, BATCH - 1]
+    xs = x[cols].cpu().numpy().astype(np.complex128)
+    ys = y[cols].cpu().numpy()
+    ref = oracle.fft_batched(xs, -1, nthreads=4)
+    rel = float(np.linalg.norm(ys - ref) / np.linalg.norm(ref))
+
+    # e2e: through the C ABI with host buffers (pinned), copies inside the timed region
+    hx = x.cpu().pin_memory()
+    hy = torch.empty_like(hx).pin_memory()
+    hxn, hyn = hx.numpy(), hy.numpy()
+    ph = F.plan_fft(hxn.T, 1)
+
+    def e2e_step():
+        F.mul_(hyn.T, ph, hxn.T)
+
+    e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    e2e_steps = max(3, min(args.steps, 10))
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_dt = (time.perf_counter() - t0) / e2e_steps
+    e2e_dt = max_over_ranks(e2e_dt)
+    e2e_value = total_flops / e2e_dt / 1e9
+
+    extra = {}
+    if not args.no_extra and rank == 0:
+        for (n2, b2) in EXTRA:
+            xe = torch.complex(torch.randn(b2, n2, device=dev), torch.randn(b2, n2, device=dev))
+            ye = torch.empty_like(xe)
+            pe = F.plan_fft(xe.T, 1)
+            for _ in range(3):
+                F.mul_(ye.T, pe, xe.T)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(10):
+                F.mul_(ye.T, pe, xe.T)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1) / 10
+            extra[f"c32_n{n2}_b{b2}"] = {
+                "ms": t, "GFLOP/s": flops(n2, b2) / (t * 1e-3) / 1e9,
+                "GB/s": 2.0 * n2 * b2 * ES / (t * 1e-3) / 1e9, "schedule": pe.describe(xe.T)}
+            del xe, ye, pe
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        nthreads = os.cpu_count() or 1
+        sample = 2048
+        v, dt = cpu_baseline(N, sample, nthreads)
+        cpu = {"value": v, "unit": "GFLOP/s", "cores": nthreads, "kind": "port",
+               "sample": f"{sample} transforms of C32 N={N} (of the {BATCH}-column batch), "
+                         f"split over {nthreads} threads, {dt:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": "batched FFT GFLOP/s (5 N log2 N), C32 N=4096 x 16384",
+            "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"batched C32 forward FFT, N={N}, {BATCH} contiguous columns "
+                                   "per GPU", "n": N, "batch_per_gpu": BATCH,
+                       "parallelism": f"batch-sharded x{world} (no collective)",
+                       "l2": "inputs and outputs (512 MiB each) larger than L2; no flush",
+                       "schedule": p.describe(xt)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "alg_bytes_per_launch": alg_bytes, "traffic": None},
+            "hbm_gbs": achieved,
+            "rel_l2_vs_fp64_oracle": rel,
+            "e2e": {"value": e2e_value, "unit": "GFLOP/s",
+                    "h2d_bytes_per_step": int(N * BATCH * ES),
+                    "d2h_bytes_per_step": int(N * BATCH * ES),
+                    "path": "fb_execute_host from pinned host memory"},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+            "extra": extra,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,87 @@
+// fb_internal.h -- structures shared by the planner (fb_plan.cu) and the
+// kernels (fb_kernels.cu).  Not part of the public C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define FB_MAX_STAGES 24
+#define FB_MAX_PRIME 71  // largest prime done by a register butterfly
+
+namespace fb {
+
+// How one side (load or store) of a line kernel addresses memory.
+// Line l is split as l0 = l % m0, t = l / m0, l1 = t % m1, l2 = t / m1; its
+// base offset is l0*s0 + l1*s1 + l2*s2 elements and element i of the line is at
+// base + i*es.  `vn`, `ves`, `vls`: element i of line l is present when
+// i*ves + l0*vls < vn (absent loads read zero, absent stores are skipped);
+// the same index selects the optional multiplier table `mul`.
+struct LineIO {
+  int64_t s0, s1, s2, es;
+  int64_t vn, ves, vls;
+  const void* mul;  // per-element multiplier (chirp) or null
+  int mode;         // 0: line-major (a line's threads walk its elements),
+                    // 1: element-major (threads walk the G lines of a block first)
+  int count;        // elements touched per line (<= L)
+};
+
+// A stage program: Stockham passes with the given radices, the per-stage
+// twiddle tables at tw + tw_off[s] (entries k*(R-1) + r-1 = w_P^(r k),
+// P = Ns*R, forward sign).
+struct StageProg {
+  int L;
+  int nst;
+  int radix[FB_MAX_STAGES];
+  int tw_off[FB_MAX_STAGES];
+  const void* tw;
+};
+
+struct LineArgs {
+  const void* in;
+  void* out;
+  int64_t nlines, m0, m1;
+  LineIO ld, st;
+  StageProg prog;
+  int dir1;             // direction of the first transform (-1 / +1)
+  int dir2;             // direction of the second (only with mid)
+  const void* mid;      // pointwise multiplier between the two transforms, or null
+  int64_t mid_ls, mid_es;
+  // twiddle on store: multiply element k of line l by w_N^(dir * l0 * k),
+  // w_N^e = hi[e >> shift] * lo[e & (2^shift - 1)].
+  int64_t tw_N;         // 0: none
+  int tw_dir, tw_shift;
+  const void* tw_hi;
+  const void* tw_lo;
+  double scale;         // applied on store when != 1
+  int G, T;             // lines per block, threads per line
+  int Lpad;             // smem elements per line
+  const void* prime_cs; // cos/sin tables of odd primes (see prime_table_offset)
+  int* err;             // device flag: set to the radix when a program names one
+                        // this kernel has no butterfly for (never traps)
+};
+
+// Offsets (in (cos,sin) pairs) of each odd prime's table inside prime_cs.
+int prime_table_offset(int p);
+int prime_table_total();
+
+// Kernel launch entry points (fb_kernels.cu).  dtype: 0 = C32, 1 = C64.
+cudaError_t launch_line(int dtype, int variant, const LineArgs& a, cudaStream_t s);
+size_t line_smem_bytes(int dtype, const LineArgs& a);
+int line_max_threads();
+// variant bits: 1 = large register budget (32 values/thread), 2 = big primes
+cudaError_t gen_stage_twiddles(int dtype, void* out, int R, int64_t Ns, cudaStream_t s);
+// out[q] = exp(sign * 2 pi i * ((q*step) mod N) / N) for q < count, sign = -1
+cudaError_t gen_roots(int dtype, void* out, int64_t N, int64_t step, int64_t count,
+                      cudaStream_t s);
+// Bluestein chirp pieces for length N, pad M, direction dir (FFTA
+// src/algos.jl:344-367: b[n] = exp(i pi sgn n^2 / N), sgn = -dir):
+//   pre[n]  = conj(b[n])            n < N
+//   post[n] = conj(b[n]) (scaled by 1/M when post_scale)  n < N
+//   bext[m] = b[m] (m < N), b[M-m] at M-m (0 < m < N), 0 elsewhere
+cudaError_t gen_chirp(int dtype, void* pre, void* post, void* bext_c64, int64_t N, int64_t M,
+                      int dir, cudaStream_t s);
+// Round a C64 array to the plan's type (copy for C64).
+cudaError_t convert_c64(int dtype, void* dst, const void* src_c64, int64_t n, double scale,
+                        cudaStream_t s);
+cudaError_t gen_prime_tables(void* f32tab, void* f64tab, cudaStream_t s);
+
+}  // namespace fb

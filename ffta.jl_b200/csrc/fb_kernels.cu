@@ -1,0 +1,231 @@
+// fb_kernels.cu -- line-kernel dispatch and the FP64 table generators.
+//
+// A "line" is one 1-D transform of length L held in shared memory.  A block
+// holds G lines; each line is processed by T threads.  The kernel
+//   1. loads its lines (gathering strided elements, zero-filling absent ones,
+//      multiplying by an optional per-element table -- the Bluestein chirp),
+//   2. runs a Stockham stage program in shared memory (radix 2/3/4/5/8/16
+//      and odd-prime butterflies up to 71), in place: every stage reads its
+//      butterflies into registers, synchronises, then writes,
+//   3. optionally multiplies by a pointwise table and runs a second program in
+//      the opposite direction (the Bluestein convolution in one kernel),
+//   4. stores, fusing the four-step twiddle, an optional per-element table
+//      and a scale factor.
+// The same kernel serves batched 1-D columns, strided N-D axes, both passes
+// of the four-step and all three passes of the multi-pass Bluestein.
+//
+// The reference computes all of this on the CPU with recursive radix-4 /
+// radix-3 / DFT / Bluestein functions (FFTA src/algos.jl:51-424) and a
+// Singleton twiddle recurrence (src/singleton_twiddle.jl:25-39); here every
+// twiddle comes from a table computed in FP64 and rounded once.
+#include <cuda_runtime.h>
+
+#include "fb_device.cuh"
+#include "fb_internal.h"
+
+namespace fb {
+
+// ------------------------------------------------------------ prime tables
+static const int kPrimes[] = {7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53, 59, 61, 67, 71};
+static const int kNumPrimes = sizeof(kPrimes) / sizeof(kPrimes[0]);
+
+int prime_table_offset(int p) {
+  int off = 0;
+  for (int i = 0; i < kNumPrimes; ++i) {
+    if (kPrimes[i] == p) return off;
+    off += kPrimes[i];
+  }
+  return -1;
+}
+int prime_table_total() {
+  int off = 0;
+  for (int i = 0; i < kNumPrimes; ++i) off += kPrimes[i];
+  return off;
+}
+
+cudaError_t launch_line_f32_c16(const LineArgs&, size_t, cudaStream_t);
+cudaError_t launch_line_f32_c32(const LineArgs&, size_t, cudaStream_t);
+cudaError_t launch_line_f32_big(const LineArgs&, size_t, cudaStream_t);
+cudaError_t launch_line_f64_c16(const LineArgs&, size_t, cudaStream_t);
+cudaError_t launch_line_f64_c32(const LineArgs&, size_t, cudaStream_t);
+cudaError_t launch_line_f64_big(const LineArgs&, size_t, cudaStream_t);
+
+size_t line_smem_bytes(int dtype, const LineArgs& a) {
+  const size_t es = dtype == 0 ? 8 : 16;
+  return (size_t)a.G * a.Lpad * es + (size_t)3 * a.G * sizeof(int64_t);
+}
+int line_max_threads() { return 512; }
+
+cudaError_t launch_line(int dtype, int variant, const LineArgs& a, cudaStream_t s) {
+  const size_t smem = line_smem_bytes(dtype, a);
+  const bool cap32 = variant & 1, big = variant & 2;
+  if (dtype == 0) {
+    if (big) return launch_line_f32_big(a, smem, s);
+    return cap32 ? launch_line_f32_c32(a, smem, s) : launch_line_f32_c16(a, smem, s);
+  }
+  if (big) return launch_line_f64_big(a, smem, s);
+  return cap32 ? launch_line_f64_c32(a, smem, s) : launch_line_f64_c16(a, smem, s);
+}
+
+// ------------------------------------------------------------ FP64 tables
+// exp(-2 pi i m / N) for integer m, computed in FP64: the index is reduced
+// exactly to a quadrant and a fraction <= 1/2 of it, then CUDA's sincospi.
+__device__ double2 root_fp64(int64_t m, int64_t N) {
+  m %= N;
+  if (m < 0) m += N;
+  const int64_t m4 = 4 * m;
+  const int q = (int)(m4 / N);
+  const int64_t rem = m4 - (int64_t)q * N;  // theta = (pi/2)(q + rem/N)
+  const bool flip = 2 * rem > N;
+  const int64_t rr = flip ? N - rem : rem;
+  const double x = (double)rr / (double)N;  // in [0, 1/2]
+  double s, c;
+  sincospi(0.5 * x, &s, &c);
+  const double cq = flip ? s : c, sq = flip ? c : s;  // cos, sin of (pi/2) rem/N
+  double ct, st;
+  switch (q) {
+    case 0: ct = cq; st = sq; break;
+    case 1: ct = -sq; st = cq; break;
+    case 2: ct = -cq; st = -sq; break;
+    default: ct = sq; st = -cq; break;
+  }
+  return make_double2(ct, -st);
+}
+
+template <typename C> __device__ __forceinline__ C from_d2(double2 v);
+template <> __device__ __forceinline__ float2 from_d2<float2>(double2 v) {
+  return make_float2((float)v.x, (float)v.y);
+}
+template <> __device__ __forceinline__ double2 from_d2<double2>(double2 v) { return v; }
+
+template <typename C>
+__global__ void k_stage_tw(C* out, int R, int64_t Ns, int64_t count) {
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < count;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = idx / (R - 1);
+    const int64_t r = idx % (R - 1) + 1;
+    out[idx] = from_d2<C>(root_fp64(r * k, Ns * R));
+  }
+}
+
+template <typename C>
+__global__ void k_roots(C* out, int64_t N, int64_t step, int64_t count) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < count;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned __int128 e = (unsigned __int128)q * (unsigned __int128)step;
+    out[q] = from_d2<C>(root_fp64((int64_t)(e % (unsigned __int128)N), N));
+  }
+}
+
+// b[n] = exp(i pi sgn p / N), p = n^2 mod 2N (exact), sgn = -dir.
+// exp(-i pi p / N) = root(p, 2N); sgn > 0 takes the conjugate.
+__device__ double2 chirp_b(int64_t n, int64_t N, int dir) {
+  const unsigned __int128 p = ((unsigned __int128)n * (unsigned __int128)n) % (unsigned __int128)(2 * N);
+  double2 r = root_fp64((int64_t)p, 2 * N);
+  if (-dir > 0) r.y = -r.y;
+  return r;
+}
+
+template <typename C>
+__global__ void k_chirp(C* pre, C* post, double2* bext, int64_t N, int64_t M, int dir) {
+  const double invM = 1.0 / (double)M;
+  for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < M;
+       m += (int64_t)gridDim.x * blockDim.x) {
+    if (m < N) {
+      const double2 b = chirp_b(m, N, dir);
+      if (pre) pre[m] = from_d2<C>(make_double2(b.x, -b.y));
+      if (post) post[m] = from_d2<C>(make_double2(b.x * invM, -b.y * invM));
+    }
+    if (bext) {
+      double2 v = make_double2(0.0, 0.0);
+      if (m < N)
+        v = chirp_b(m, N, dir);
+      else if (M - m < N)
+        v = chirp_b(M - m, N, dir);
+      bext[m] = v;
+    }
+  }
+}
+
+template <typename C>
+__global__ void k_convert(C* dst, const double2* src, int64_t n, double scale) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double2 v = src[i];
+    dst[i] = from_d2<C>(make_double2(v.x * scale, v.y * scale));
+  }
+}
+
+__global__ void k_prime_tables(float* f32, double* f64, int total) {
+  // walk the prime list: entry e belongs to prime p at offset off
+  const int primes[] = {7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53, 59, 61, 67, 71};
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    int off = 0, p = 0;
+    for (int i = 0; i < 17; ++i) {
+      if (e < off + primes[i]) { p = primes[i]; break; }
+      off += primes[i];
+    }
+    const int m = e - off;
+    const double2 r = root_fp64(m, p);  // (cos, -sin)
+    f64[2 * e] = r.x;
+    f64[2 * e + 1] = -r.y;
+    f32[2 * e] = (float)r.x;
+    f32[2 * e + 1] = (float)(-r.y);
+  }
+}
+
+static unsigned grid_for(int64_t n) {
+  int64_t b = (n + 255) / 256;
+  if (b < 1) b = 1;
+  if (b > 65535) b = 65535;
+  return (unsigned)b;
+}
+
+cudaError_t gen_stage_twiddles(int dtype, void* out, int R, int64_t Ns, cudaStream_t s) {
+  const int64_t count = (int64_t)(R - 1) * Ns;
+  if (count <= 0) return cudaSuccess;
+  if (dtype == 0)
+    k_stage_tw<float2><<<grid_for(count), 256, 0, s>>>((float2*)out, R, Ns, count);
+  else
+    k_stage_tw<double2><<<grid_for(count), 256, 0, s>>>((double2*)out, R, Ns, count);
+  return cudaGetLastError();
+}
+
+cudaError_t gen_roots(int dtype, void* out, int64_t N, int64_t step, int64_t count,
+                      cudaStream_t s) {
+  if (count <= 0) return cudaSuccess;
+  if (dtype == 0)
+    k_roots<float2><<<grid_for(count), 256, 0, s>>>((float2*)out, N, step, count);
+  else
+    k_roots<double2><<<grid_for(count), 256, 0, s>>>((double2*)out, N, step, count);
+  return cudaGetLastError();
+}
+
+cudaError_t gen_chirp(int dtype, void* pre, void* post, void* bext_c64, int64_t N, int64_t M,
+                      int dir, cudaStream_t s) {
+  if (dtype == 0)
+    k_chirp<float2><<<grid_for(M), 256, 0, s>>>((float2*)pre, (float2*)post, (double2*)bext_c64,
+                                                N, M, dir);
+  else
+    k_chirp<double2><<<grid_for(M), 256, 0, s>>>((double2*)pre, (double2*)post,
+                                                 (double2*)bext_c64, N, M, dir);
+  return cudaGetLastError();
+}
+
+cudaError_t convert_c64(int dtype, void* dst, const void* src_c64, int64_t n, double scale,
+                        cudaStream_t s) {
+  if (dtype == 0)
+    k_convert<float2><<<grid_for(n), 256, 0, s>>>((float2*)dst, (const double2*)src_c64, n, scale);
+  else
+    k_convert<double2><<<grid_for(n), 256, 0, s>>>((double2*)dst, (const double2*)src_c64, n,
+                                                   scale);
+  return cudaGetLastError();
+}
+
+cudaError_t gen_prime_tables(void* f32tab, void* f64tab, cudaStream_t s) {
+  const int total = prime_table_total();
+  k_prime_tables<<<grid_for(total), 256, 0, s>>>((float*)f32tab, (double*)f64tab, total);
+  return cudaGetLastError();
+}
+
+}  // namespace fb

@@ -1,0 +1,979 @@
+// fb_plan.cu -- planner, executor and C ABI of libfftab200.so.
+//
+// FFTA.jl plans a transform by building a call graph (src/callgraph.jl:76-126)
+// and runs it with recursive CPU kernels (src/algos.jl).  This planner keeps
+// the same inputs and semantics -- length, direction, Bluestein cutoff,
+// region -- and maps each transformed axis to a short sequence of line-kernel
+// launches (fb_kernels.cu):
+//   DIRECT  one kernel: the whole line in shared memory (lengths up to Lmax)
+//   BLUE1   one kernel: Bluestein with the pad held in shared memory
+//   FOUR    two kernels: N = N1*N2, each pass a DIRECT or BLUE1 line
+//           transform, the twiddle fused into the first pass's store
+//   BLUE3   three kernels: Bluestein whose pad M = M1*M2 is done four-step,
+//           with the chirp spectrum multiply fused between the two halves
+// The arithmetic of a length depends only on (length, type, direction,
+// cutoff), never on batch or strides, so strided and batched transforms are
+// bit-identical to single contiguous ones.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "fb_internal.h"
+#include "fftab200.h"
+
+#define FB_VERSION "fftab200 0.1.0 (sm_100a)"
+
+namespace fb {
+
+static thread_local std::string g_last_error;
+
+struct FbError {
+  int code;
+  std::string msg;
+};
+[[noreturn]] static void fail(int code, const std::string& m) { throw FbError{code, m}; }
+static void cuda_check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  cudaGetLastError();
+  if (e == cudaErrorMemoryAllocation)
+    fail(FB_ERR_OUT_OF_MEMORY, std::string(what) + ": out of device memory");
+  fail(FB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ----------------------------------------------------------- device memory
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  explicit DevBuf(size_t b) : bytes(b) {
+    if (b) cuda_check(cudaMalloc(&p, b), "cudaMalloc");
+  }
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+};
+
+// Per-device odd-prime cos/sin tables used by the register DFTs.
+struct DeviceTables {
+  void* f32 = nullptr;
+  void* f64 = nullptr;
+  int* err = nullptr;  // kernel error flag (see LineArgs::err)
+};
+static std::mutex g_dev_mu;
+static std::map<int, DeviceTables> g_dev_tables;
+
+static const DeviceTables& device_tables(int dev) {
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  auto it = g_dev_tables.find(dev);
+  if (it != g_dev_tables.end()) return it->second;
+  DeviceTables t;
+  const int total = prime_table_total();
+  cuda_check(cudaMalloc(&t.f32, (size_t)total * 2 * sizeof(float)), "cudaMalloc");
+  cuda_check(cudaMalloc(&t.f64, (size_t)total * 2 * sizeof(double)), "cudaMalloc");
+  cuda_check(cudaMalloc(&t.err, sizeof(int)), "cudaMalloc");
+  cuda_check(cudaMemset(t.err, 0, sizeof(int)), "cudaMemset");
+  cuda_check(gen_prime_tables(t.f32, t.f64, 0), "prime tables");
+  cuda_check(cudaDeviceSynchronize(), "prime tables");
+  return g_dev_tables.emplace(dev, t).first->second;
+}
+
+// ------------------------------------------------------------ arithmetic
+static int64_t ipow2_ceil(int64_t v) {
+  int64_t p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+static std::vector<std::pair<int64_t, int>> factorize(int64_t n) {
+  std::vector<std::pair<int64_t, int>> f;
+  for (int64_t d = 2; d * d <= n; d += (d == 2 ? 1 : 2)) {
+    int c = 0;
+    while (n % d == 0) {
+      n /= d;
+      ++c;
+    }
+    if (c) f.push_back({d, c});
+  }
+  if (n > 1) f.push_back({n, 1});
+  return f;
+}
+static bool is_prime(int64_t n) {
+  if (n < 2) return false;
+  auto f = factorize(n);
+  return f.size() == 1 && f[0].second == 1;
+}
+static int elem_bytes(int dtype) { return dtype == FB_C32 ? 8 : 16; }
+static int64_t lmax_for(int dtype) { return dtype == FB_C32 ? 16384 : 8192; }
+
+// ------------------------------------------------------ line transforms
+// A transform of one line done by one kernel.
+struct LineX {
+  int kind = 0;  // 0 direct, 1 Bluestein in shared memory
+  int64_t n = 0; // logical length
+  int L = 0;     // shared-memory transform length (n, or the Bluestein pad)
+  std::vector<int> radices;
+  int variant = 0;
+  int T = 1;
+  std::vector<int> tw_off;
+  int64_t tw_count = 0;
+};
+
+static int um_for(int R, int cap) { return R >= cap ? 1 : cap / R; }
+
+// Radix program for a length whose prime factors are all <= FB_MAX_PRIME:
+// powers of two as radix 16 with an 8, 4 or 2 (8*4 in place of 16*2), then
+// threes, fives and the odd primes in ascending order.
+static std::vector<int> radix_program(int64_t L) {
+  std::vector<int> r;
+  int a = 0;
+  while (L % 2 == 0) {
+    L /= 2;
+    ++a;
+  }
+  int q = a / 4, rem = a % 4;
+  if (rem == 1 && q >= 1) {
+    for (int i = 0; i < q - 1; ++i) r.push_back(16);
+    r.push_back(8);
+    r.push_back(4);
+  } else {
+    for (int i = 0; i < q; ++i) r.push_back(16);
+    if (rem == 1) r.push_back(2);
+    if (rem == 2) r.push_back(4);
+    if (rem == 3) r.push_back(8);
+  }
+  for (auto& pe : factorize(L))
+    for (int i = 0; i < pe.second; ++i) r.push_back((int)pe.first);
+  return r;
+}
+
+// Can `n` be a DIRECT line (all factors by register butterflies) under the
+// Bluestein cutoff?  FFTA sends a prime p >= 5 to Bluestein when
+// p >= cutoff; 2 and 3 always take the radix kernels (src/callgraph.jl:86-100).
+static bool direct_ok(int64_t n, int64_t cutoff, int dtype) {
+  if (n < 1 || n > lmax_for(dtype)) return false;
+  for (auto& pe : factorize(n)) {
+    const int64_t p = pe.first;
+    if (p == 2 || p == 3) continue;
+    if (p > FB_MAX_PRIME || p >= cutoff) return false;
+  }
+  return true;
+}
+
+// Threads per line and the kernel variant for a radix program.
+static bool pick_threads(int L, const std::vector<int>& rad, int* T_out, int* variant_out) {
+  bool big = false;
+  for (int R : rad) big |= R > 16;
+  const int caps[2] = {16, 32};
+  for (int ci = 0; ci < 2; ++ci) {
+    const int cap = caps[ci];
+    if (big && cap != 16) break;
+    int tmin = 1;
+    for (int R : rad) {
+      const int nb = L / R;
+      const int need = (nb + um_for(R, cap) - 1) / um_for(R, cap);
+      tmin = std::max(tmin, need);
+    }
+    if (tmin <= line_max_threads()) {
+      int T;
+      if (tmin <= 32) {
+        T = 1;
+        while (T < tmin) T <<= 1;
+      } else {
+        T = (tmin + 31) / 32 * 32;
+      }
+      *T_out = T;
+      *variant_out = (cap == 32 ? 1 : 0) | (big ? 2 : 0);
+      return true;
+    }
+  }
+  return false;
+}
+
+static bool make_direct(int64_t n, int64_t cutoff, int dtype, LineX* x) {
+  if (!direct_ok(n, cutoff, dtype)) return false;
+  LineX r;
+  r.kind = 0;
+  r.n = n;
+  r.L = (int)n;
+  r.radices = radix_program(n);
+  if (!pick_threads(r.L, r.radices, &r.T, &r.variant)) return false;
+  *x = r;
+  return true;
+}
+
+static bool make_blue1(int64_t n, int dtype, LineX* x) {
+  const int64_t M = ipow2_ceil(2 * n - 1);  // FFTA's pad, src/algos.jl:345
+  if (M > lmax_for(dtype)) return false;
+  LineX r;
+  if (!make_direct(M, 1 << 30, dtype, &r)) return false;
+  r.kind = 1;
+  r.n = n;
+  *x = r;
+  return true;
+}
+
+// One line transform of length n if one kernel can do it.
+static bool make_line(int64_t n, int64_t cutoff, int dtype, LineX* x) {
+  if (make_direct(n, cutoff, dtype, x)) return true;
+  // Lengths with a factor that needs Bluestein, and primes >= cutoff.
+  return make_blue1(n, dtype, x);
+}
+
+static double line_cost(const LineX& x) {
+  const double L = x.L;
+  const double c = L * (std::log2(std::max(2.0, L)) + 4.0);
+  return x.kind == 0 ? c : 2.0 * c + 2.0 * L;
+}
+
+// ------------------------------------------------------------------ plan
+enum BufId { B_IN = 0, B_OUT = 1, B_S0 = 2, B_S1 = 3 };
+
+struct Pass {
+  LineArgs a;
+  int variant = 0;
+  int src = B_IN, dst = B_OUT;
+  std::string what;
+};
+
+struct BDim {
+  int64_t n, is, os;
+};
+
+struct Axis {
+  int64_t n = 0;
+  std::string kind;
+  std::vector<Pass> passes;
+  std::vector<BDim> outer;  // batch dims looped on the host
+};
+
+}  // namespace fb
+
+struct fb_plan_s {
+  int dtype = 0, dir = -1, device = 0;
+  int64_t cutoff = 73;
+  double scale = 1.0;
+  int rank = 0;
+  std::vector<int64_t> dims, istrides, ostrides;
+  std::vector<int> region;  // 0-based, ascending
+  std::vector<fb::Axis> axes;
+  std::vector<std::unique_ptr<fb::DevBuf>> bufs;  // tables
+  size_t scratch_elems = 0;
+  std::unique_ptr<fb::DevBuf> scratch0, scratch1;
+  // host-execution staging
+  std::unique_ptr<fb::DevBuf> hin, hout;
+  int64_t in_span = 0, out_span = 0;
+  size_t table_bytes = 0;
+};
+
+namespace fb {
+
+static void* alloc_table(fb_plan_s* P, size_t bytes) {
+  P->bufs.emplace_back(new DevBuf(bytes));
+  P->table_bytes += bytes;
+  return P->bufs.back()->p;
+}
+
+static void fill_prog(fb_plan_s* P, LineX& x, StageProg* prog) {
+  if ((int)x.radices.size() > FB_MAX_STAGES) fail(FB_ERR_UNSUPPORTED, "too many stages");
+  // stage twiddle table: stage s has (R-1)*Ns entries
+  int64_t off = 0, Ns = 1;
+  x.tw_off.clear();
+  for (int R : x.radices) {
+    x.tw_off.push_back((int)off);
+    off += (int64_t)(R - 1) * Ns;
+    Ns *= R;
+  }
+  x.tw_count = off;
+  void* tw = nullptr;
+  if (off > 0) {
+    tw = alloc_table(P, (size_t)off * elem_bytes(P->dtype));
+    Ns = 1;
+    for (size_t s = 0; s < x.radices.size(); ++s) {
+      const int R = x.radices[s];
+      cuda_check(gen_stage_twiddles(P->dtype, (char*)tw + (size_t)x.tw_off[s] * elem_bytes(P->dtype),
+                                    R, Ns, 0),
+                 "stage twiddles");
+      Ns *= R;
+    }
+  }
+  memset(prog, 0, sizeof(*prog));
+  prog->L = x.L;
+  prog->nst = (int)x.radices.size();
+  for (size_t s = 0; s < x.radices.size(); ++s) {
+    prog->radix[s] = x.radices[s];
+    prog->tw_off[s] = x.tw_off[s];
+  }
+  prog->tw = tw;
+}
+
+static fb_plan_s* create_plan(int dtype, int dir, int rank, const int64_t* dims,
+                              const int64_t* istrides, const int64_t* ostrides,
+                              const std::vector<int>& region, int64_t cutoff);
+static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s);
+
+// Chirp spectrum FFT_M(b_ext), forward, computed in FP64 by a C64 plan and
+// rounded to the plan type, optionally scaled.
+static void* chirp_spectrum(fb_plan_s* P, int64_t N, int64_t M, double scale) {
+  DevBuf bext((size_t)M * 16), spec((size_t)M * 16);
+  cuda_check(gen_chirp(P->dtype, nullptr, nullptr, bext.p, N, M, P->dir, 0), "chirp");
+  std::vector<int> reg{0};
+  int64_t d[1] = {M}, st[1] = {1};
+  std::unique_ptr<fb_plan_s> sub(create_plan(FB_C64, FB_FORWARD, 1, d, st, st, reg, 1 << 30));
+  execute_plan(sub.get(), bext.p, spec.p, 0);
+  void* mid = alloc_table(P, (size_t)M * elem_bytes(P->dtype));
+  cuda_check(convert_c64(P->dtype, mid, spec.p, M, scale, 0), "chirp spectrum");
+  cuda_check(cudaDeviceSynchronize(), "chirp spectrum");
+  return mid;
+}
+
+// Tables of a Bluestein line: pre = conj(b), post = conj(b)/M, mid = FFT(b_ext).
+static void blue_tables(fb_plan_s* P, int64_t N, int64_t M, void** pre, void** post, void** mid) {
+  *pre = alloc_table(P, (size_t)N * elem_bytes(P->dtype));
+  *post = alloc_table(P, (size_t)N * elem_bytes(P->dtype));
+  cuda_check(gen_chirp(P->dtype, *pre, *post, nullptr, N, M, P->dir, 0), "chirp");
+  *mid = chirp_spectrum(P, N, M, 1.0);
+}
+
+static int pick_G(const fb_plan_s* P, int L, int T, int Lpad, bool elem_major, int64_t nlines) {
+  const int es = elem_bytes(P->dtype);
+  const int thr_cap = std::max(1, line_max_threads() / T);
+  const size_t line_bytes = (size_t)Lpad * es + 24;
+  const size_t budget = 100 * 1024;
+  int g_smem = (int)std::max<size_t>(1, budget / line_bytes);
+  int want = std::max(1, 256 / T);
+  if (elem_major) want = std::max(want, es == 8 ? 16 : 8);
+  int G = std::min(std::min(thr_cap, g_smem), want);
+  int64_t nl = std::max<int64_t>(1, nlines);
+  while (G > 1 && G / 2 >= nl) G /= 2;
+  if (elem_major) {
+    int p = 1;
+    while (p * 2 <= G) p *= 2;
+    G = p;
+  }
+  (void)L;
+  return std::max(1, G);
+}
+
+static int lpad_for(int L) {
+  int lp = (L - 1) + ((L - 1) >> 4) + 1;
+  if (lp < 1) lp = 1;
+  if ((lp & 1) == 0) lp += 1;
+  return lp;
+}
+
+static LineIO io_plain(int64_t s0, int64_t s1, int64_t s2, int64_t es, int count) {
+  LineIO io;
+  memset(&io, 0, sizeof(io));
+  io.s0 = s0;
+  io.s1 = s1;
+  io.s2 = s2;
+  io.es = es;
+  io.vn = INT64_MAX;
+  io.ves = 0;
+  io.vls = 0;
+  io.mul = nullptr;
+  io.mode = 0;
+  io.count = count;
+  return io;
+}
+
+// Base LineArgs for a line transform `x` applied to `nlines` lines.
+static void base_args(fb_plan_s* P, LineX& x, LineArgs* a, int dir) {
+  memset(a, 0, sizeof(*a));
+  fill_prog(P, x, &a->prog);
+  a->dir1 = dir;
+  a->dir2 = dir;
+  a->scale = 1.0;
+  a->T = x.T;
+  a->Lpad = lpad_for(x.L);
+  const DeviceTables& dt = device_tables(P->device);
+  a->prime_cs = P->dtype == FB_C32 ? dt.f32 : dt.f64;
+  a->err = dt.err;
+  a->m0 = 1;
+  a->m1 = 1;
+}
+
+// Make `x` a Bluestein line on top of base args: pre on load, convolution,
+// post on store.  `vls_ld/vls_st`, `ves` describe the element index as in LineIO.
+static void attach_blue(fb_plan_s* P, const LineX& x, LineArgs* a) {
+  void *pre, *post, *mid;
+  blue_tables(P, x.n, x.L, &pre, &post, &mid);
+  a->ld.mul = pre;
+  a->ld.vn = x.n;
+  a->ld.ves = 1;
+  a->ld.vls = 0;
+  a->ld.count = (int)x.n;
+  a->st.mul = post;
+  a->st.vn = x.n;
+  a->st.ves = 1;
+  a->st.vls = 0;
+  a->st.count = (int)x.n;
+  a->mid = mid;
+  a->mid_ls = 0;
+  a->mid_es = 1;
+  a->dir1 = FB_FORWARD;
+  a->dir2 = FB_BACKWARD;
+}
+
+// Two-level root tables for w_N^e, e < N: hi[e >> shift] * lo[e & mask].
+static void attach_twiddle(fb_plan_s* P, LineArgs* a, int64_t N, int dir) {
+  int shift = 0;
+  while ((int64_t(1) << (2 * shift)) < N) ++shift;  // 2^shift >= sqrt(N)
+  const int64_t lo_n = int64_t(1) << shift;
+  const int64_t hi_n = (N + lo_n - 1) / lo_n;
+  void* lo = alloc_table(P, (size_t)lo_n * elem_bytes(P->dtype));
+  void* hi = alloc_table(P, (size_t)hi_n * elem_bytes(P->dtype));
+  cuda_check(gen_roots(P->dtype, lo, N, 1, lo_n, 0), "roots");
+  cuda_check(gen_roots(P->dtype, hi, N, lo_n, hi_n, 0), "roots");
+  a->tw_N = N;
+  a->tw_dir = dir;
+  a->tw_shift = shift;
+  a->tw_lo = lo;
+  a->tw_hi = hi;
+}
+
+// Collapse batch dims that are contiguous in both input and output, drop
+// extent-1 dims, and order them by input stride.
+static std::vector<BDim> normalize_batch(std::vector<BDim> bd) {
+  std::vector<BDim> v;
+  for (auto& b : bd)
+    if (b.n != 1) v.push_back(b);
+  std::sort(v.begin(), v.end(), [](const BDim& x, const BDim& y) {
+    return std::llabs(x.is) < std::llabs(y.is);
+  });
+  bool merged = true;
+  while (merged) {
+    merged = false;
+    for (size_t i = 0; i + 1 < v.size() && !merged; ++i) {
+      BDim& a = v[i];
+      BDim& b = v[i + 1];
+      if (a.is * a.n == b.is && a.os * a.n == b.os) {
+        a.n *= b.n;
+        v.erase(v.begin() + i + 1);
+        merged = true;
+      }
+    }
+  }
+  return v;
+}
+
+static int64_t prod_n(const std::vector<BDim>& v, size_t from, size_t to) {
+  int64_t p = 1;
+  for (size_t i = from; i < to && i < v.size(); ++i) p *= v[i].n;
+  return p;
+}
+
+// Split batch dims into kernel levels (up to `kl`) and host-looped dims.
+static void split_levels(const std::vector<BDim>& bd, size_t kl, std::vector<BDim>* inner,
+                         std::vector<BDim>* outer) {
+  inner->clear();
+  outer->clear();
+  for (size_t i = 0; i < bd.size(); ++i) (i < kl ? inner : outer)->push_back(bd[i]);
+}
+
+static int64_t level_n(const std::vector<BDim>& v, size_t i) { return i < v.size() ? v[i].n : 1; }
+static int64_t level_is(const std::vector<BDim>& v, size_t i) { return i < v.size() ? v[i].is : 0; }
+static int64_t level_os(const std::vector<BDim>& v, size_t i) { return i < v.size() ? v[i].os : 0; }
+
+static Axis plan_direct_axis(fb_plan_s* P, int64_t n, LineX& x, int64_t is, int64_t os,
+                             const std::vector<BDim>& bd, int src, int dst) {
+  Axis ax;
+  ax.n = n;
+  std::vector<BDim> inner;
+  split_levels(bd, 3, &inner, &ax.outer);
+  Pass p;
+  base_args(P, x, &p.a, P->dir);
+  p.variant = x.variant;
+  p.src = src;
+  p.dst = dst;
+  const int64_t nl = prod_n(inner, 0, 3);
+  p.a.nlines = nl;
+  p.a.m0 = level_n(inner, 0);
+  p.a.m1 = level_n(inner, 1);
+  p.a.ld = io_plain(level_is(inner, 0), level_is(inner, 1), level_is(inner, 2), is, (int)x.L);
+  p.a.st = io_plain(level_os(inner, 0), level_os(inner, 1), level_os(inner, 2), os, (int)x.L);
+  if (x.kind == 1) attach_blue(P, x, &p.a);
+  const bool ld_em = is != 1 && !inner.empty() && inner[0].is == 1;
+  const bool st_em = os != 1 && !inner.empty() && inner[0].os == 1;
+  p.a.ld.mode = ld_em ? 1 : 0;
+  p.a.st.mode = st_em ? 1 : 0;
+  p.a.G = pick_G(P, x.L, x.T, p.a.Lpad, ld_em || st_em, nl);
+  ax.kind = x.kind == 0 ? "DIRECT" : "BLUE1";
+  std::ostringstream w;
+  w << ax.kind << "(L=" << x.L << " radices=";
+  for (size_t i = 0; i < x.radices.size(); ++i) w << (i ? "x" : "") << x.radices[i];
+  w << " T=" << x.T << " G=" << p.a.G << " var=" << x.variant << ")";
+  p.what = w.str();
+  ax.passes.push_back(p);
+  return ax;
+}
+
+// Four-step N = N1*N2: pass 1 transforms the N2 strided columns (length N1)
+// into scratch with the twiddle w_N^(n2 k1) fused; pass 2 transforms the N1
+// rows (length N2) and writes X[k1 + N1 k2].
+static Axis plan_four_axis(fb_plan_s* P, int64_t N, int64_t N1, int64_t N2, LineX& x1, LineX& x2,
+                           int64_t is, int64_t os, const std::vector<BDim>& bd, int src, int dst) {
+  Axis ax;
+  ax.n = N;
+  ax.kind = "FOUR";
+  std::vector<BDim> inner;
+  split_levels(bd, 2, &inner, &ax.outer);
+  const int64_t B = prod_n(inner, 0, 2), B0 = level_n(inner, 0);
+  P->scratch_elems = std::max<size_t>(P->scratch_elems, (size_t)(N * B));
+  // pass 1
+  Pass p1;
+  base_args(P, x1, &p1.a, P->dir);
+  p1.variant = x1.variant;
+  p1.src = src;
+  p1.dst = B_S0;
+  p1.a.nlines = N2 * B;
+  p1.a.m0 = N2;
+  p1.a.m1 = B0;
+  p1.a.ld = io_plain(is, level_is(inner, 0), level_is(inner, 1), N2 * is, x1.L);
+  p1.a.st = io_plain(1, N, B0 * N, N2, x1.L);
+  if (x1.kind == 1) attach_blue(P, x1, &p1.a);
+  attach_twiddle(P, &p1.a, N, P->dir);
+  p1.a.ld.mode = is == 1 ? 1 : 0;
+  p1.a.st.mode = 1;
+  p1.a.G = pick_G(P, x1.L, x1.T, p1.a.Lpad, true, p1.a.nlines);
+  // pass 2
+  Pass p2;
+  base_args(P, x2, &p2.a, P->dir);
+  p2.variant = x2.variant;
+  p2.src = B_S0;
+  p2.dst = dst;
+  p2.a.nlines = N1 * B;
+  p2.a.m0 = N1;
+  p2.a.m1 = B0;
+  p2.a.ld = io_plain(N2, N, B0 * N, 1, x2.L);
+  p2.a.st = io_plain(os, level_os(inner, 0), level_os(inner, 1), N1 * os, x2.L);
+  if (x2.kind == 1) attach_blue(P, x2, &p2.a);
+  p2.a.ld.mode = 0;
+  p2.a.st.mode = os == 1 ? 1 : 0;
+  p2.a.G = pick_G(P, x2.L, x2.T, p2.a.Lpad, p2.a.st.mode == 1, p2.a.nlines);
+  std::ostringstream w1, w2;
+  w1 << "FOUR.1(N1=" << N1 << (x1.kind ? " blue" : "") << " L=" << x1.L << " T=" << x1.T
+     << " G=" << p1.a.G << ")";
+  w2 << "FOUR.2(N2=" << N2 << (x2.kind ? " blue" : "") << " L=" << x2.L << " T=" << x2.T
+     << " G=" << p2.a.G << ")";
+  p1.what = w1.str();
+  p2.what = w2.str();
+  ax.passes.push_back(p1);
+  ax.passes.push_back(p2);
+  return ax;
+}
+
+// Bluestein with the pad M = M1*M2 done four-step in three passes:
+//  1. a = x conj(b) (zero beyond N), FFT over n1 (length M1), twiddle, -> S0
+//  2. FFT over n2 (M2), times FFT(b_ext), inverse FFT over k2, twiddle, -> S1
+//  3. inverse FFT over k1 (M1), times conj(b)/M, store n < N.
+static Axis plan_blue3_axis(fb_plan_s* P, int64_t N, int64_t is, int64_t os,
+                            const std::vector<BDim>& bd, int src, int dst) {
+  const int64_t M = ipow2_ceil(2 * N - 1);
+  // balanced power-of-two split
+  int lg = 0;
+  while ((int64_t(1) << lg) < M) ++lg;
+  const int64_t M1 = int64_t(1) << (lg / 2), M2 = M / M1;
+  LineX x1, x2;
+  if (!make_direct(M1, 1 << 30, P->dtype, &x1) || !make_direct(M2, 1 << 30, P->dtype, &x2))
+    fail(FB_ERR_UNSUPPORTED, "length " + std::to_string(N) + " is beyond this build's schedules");
+  Axis ax;
+  ax.n = N;
+  ax.kind = "BLUE3";
+  std::vector<BDim> inner;
+  split_levels(bd, 2, &inner, &ax.outer);
+  const int64_t B = prod_n(inner, 0, 2), B0 = level_n(inner, 0);
+  P->scratch_elems = std::max<size_t>(P->scratch_elems, (size_t)(M * B));
+  void* pre = alloc_table(P, (size_t)N * elem_bytes(P->dtype));
+  void* post = alloc_table(P, (size_t)N * elem_bytes(P->dtype));
+  cuda_check(gen_chirp(P->dtype, pre, post, nullptr, N, M, P->dir, 0), "chirp");
+  void* mid = chirp_spectrum(P, N, M, 1.0);
+  // pass 1
+  Pass p1;
+  base_args(P, x1, &p1.a, FB_FORWARD);
+  p1.variant = x1.variant;
+  p1.src = src;
+  p1.dst = B_S0;
+  p1.a.nlines = M2 * B;
+  p1.a.m0 = M2;
+  p1.a.m1 = B0;
+  p1.a.ld = io_plain(is, level_is(inner, 0), level_is(inner, 1), M2 * is, (int)M1);
+  p1.a.ld.mul = pre;
+  p1.a.ld.vn = N;
+  p1.a.ld.ves = M2;
+  p1.a.ld.vls = 1;
+  p1.a.st = io_plain(1, M, B0 * M, M2, (int)M1);
+  attach_twiddle(P, &p1.a, M, FB_FORWARD);
+  p1.a.ld.mode = is == 1 ? 1 : 0;
+  p1.a.st.mode = 1;
+  p1.a.G = pick_G(P, x1.L, x1.T, p1.a.Lpad, true, p1.a.nlines);
+  // pass 2
+  Pass p2;
+  base_args(P, x2, &p2.a, FB_FORWARD);
+  p2.variant = x2.variant;
+  p2.src = B_S0;
+  p2.dst = B_S1;
+  p2.a.nlines = M1 * B;
+  p2.a.m0 = M1;
+  p2.a.m1 = B0;
+  p2.a.ld = io_plain(M2, M, B0 * M, 1, (int)M2);
+  p2.a.st = io_plain(1, M, B0 * M, M1, (int)M2);
+  p2.a.mid = mid;
+  p2.a.mid_ls = 1;
+  p2.a.mid_es = M1;
+  p2.a.dir1 = FB_FORWARD;
+  p2.a.dir2 = FB_BACKWARD;
+  attach_twiddle(P, &p2.a, M, FB_BACKWARD);
+  p2.a.ld.mode = 0;
+  p2.a.st.mode = 1;
+  p2.a.G = pick_G(P, x2.L, x2.T, p2.a.Lpad, true, p2.a.nlines);
+  // pass 3
+  Pass p3;
+  base_args(P, x1, &p3.a, FB_BACKWARD);
+  p3.variant = x1.variant;
+  p3.src = B_S1;
+  p3.dst = dst;
+  p3.a.nlines = M2 * B;
+  p3.a.m0 = M2;
+  p3.a.m1 = B0;
+  p3.a.ld = io_plain(M1, M, B0 * M, 1, (int)M1);
+  p3.a.st = io_plain(os, level_os(inner, 0), level_os(inner, 1), M2 * os, (int)M1);
+  p3.a.st.mul = post;
+  p3.a.st.vn = N;
+  p3.a.st.ves = M2;
+  p3.a.st.vls = 1;
+  p3.a.ld.mode = 0;
+  p3.a.st.mode = os == 1 ? 1 : 0;
+  p3.a.G = pick_G(P, x1.L, x1.T, p3.a.Lpad, p3.a.st.mode == 1, p3.a.nlines);
+  std::ostringstream w;
+  w << "BLUE3(N=" << N << " M=" << M1 << "x" << M2 << ")";
+  p1.what = w.str() + ".1";
+  p2.what = w.str() + ".2";
+  p3.what = w.str() + ".3";
+  ax.passes.push_back(p1);
+  ax.passes.push_back(p2);
+  ax.passes.push_back(p3);
+  return ax;
+}
+
+static Axis plan_axis(fb_plan_s* P, int64_t n, int64_t is, int64_t os, std::vector<BDim> bd,
+                      int src, int dst) {
+  if (n <= 0) fail(FB_ERR_DIMENSION_MISMATCH, "Array length must be strictly positive");
+  bd = normalize_batch(bd);
+  LineX x;
+  if (make_direct(n, P->cutoff, P->dtype, &x)) return plan_direct_axis(P, n, x, is, os, bd, src, dst);
+  // Bluestein for a prime in one kernel when its pad fits.
+  if (is_prime(n) && make_blue1(n, P->dtype, &x))
+    return plan_direct_axis(P, n, x, is, os, bd, src, dst);
+  // Four-step over the cheapest split into two one-kernel line transforms.
+  double best = 1e300;
+  int64_t bN1 = 0;
+  LineX b1, b2;
+  for (int64_t N1 = 2; N1 * N1 <= n; ++N1) {
+    if (n % N1) continue;
+    const int64_t cand[2] = {N1, n / N1};
+    for (int o = 0; o < 2; ++o) {
+      const int64_t a = cand[o], b = n / a;
+      LineX xa, xb;
+      if (!make_line(a, P->cutoff, P->dtype, &xa) || !make_line(b, P->cutoff, P->dtype, &xb)) continue;
+      double c = line_cost(xa) * (double)b + line_cost(xb) * (double)a;
+      // prefer balanced direct splits on ties
+      c *= 1.0 + 1e-9 * std::fabs(std::log((double)a) - std::log((double)b));
+      if (c < best) {
+        best = c;
+        bN1 = a;
+        b1 = xa;
+        b2 = xb;
+      }
+    }
+  }
+  if (bN1) return plan_four_axis(P, n, bN1, n / bN1, b1, b2, is, os, bd, src, dst);
+  return plan_blue3_axis(P, n, is, os, bd, src, dst);
+}
+
+static fb_plan_s* create_plan(int dtype, int dir, int rank, const int64_t* dims,
+                              const int64_t* istrides, const int64_t* ostrides,
+                              const std::vector<int>& region, int64_t cutoff) {
+  if (dtype != FB_C32 && dtype != FB_C64)
+    fail(FB_ERR_ARGUMENT, "element type must be ComplexF32 or ComplexF64");
+  if (dir != FB_FORWARD && dir != FB_BACKWARD) fail(FB_ERR_ARGUMENT, "direction must be -1 or +1");
+  if (rank < 1) fail(FB_ERR_DIMENSION_MISMATCH, "array must have at least one dimension");
+  for (size_t i = 0; i < region.size(); ++i) {
+    if (region[i] < 0 || region[i] >= rank)
+      fail(FB_ERR_DIMENSION_MISMATCH, "Plan region is outside array dimensions.");
+    if (i && region[i] <= region[i - 1]) fail(FB_ERR_DIMENSION_MISMATCH, "Region is invalid.");
+  }
+  for (int d = 0; d < rank; ++d) {
+    if (dims[d] < 0) fail(FB_ERR_DIMENSION_MISMATCH, "negative dimension");
+    if (istrides[d] < 0 || ostrides[d] < 0) fail(FB_ERR_ARGUMENT, "negative strides are not supported");
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    fail(FB_ERR_CUDA, "no CUDA device: this library has no CPU fallback");
+  }
+  std::unique_ptr<fb_plan_s> P(new fb_plan_s());
+  P->dtype = dtype;
+  P->dir = dir;
+  P->cutoff = cutoff;
+  P->rank = rank;
+  P->dims.assign(dims, dims + rank);
+  P->istrides.assign(istrides, istrides + rank);
+  P->ostrides.assign(ostrides, ostrides + rank);
+  P->region = region;
+  cuda_check(cudaGetDevice(&P->device), "cudaGetDevice");
+  int64_t total = 1;
+  for (int d = 0; d < rank; ++d) total *= dims[d];
+  for (size_t r = 0; r < region.size(); ++r) {
+    const int d = region[r];
+    if (dims[d] <= 0) fail(FB_ERR_DIMENSION_MISMATCH, "Array length must be strictly positive");
+  }
+  P->in_span = P->out_span = 0;
+  if (total > 0) {
+    int64_t si = 1, so = 1;
+    for (int d = 0; d < rank; ++d) {
+      si += (dims[d] - 1) * istrides[d];
+      so += (dims[d] - 1) * ostrides[d];
+    }
+    P->in_span = si;
+    P->out_span = so;
+  }
+  if (total > 0) {
+    for (size_t r = 0; r < region.size(); ++r) {
+      const int d = region[r];
+      const bool first = r == 0;
+      std::vector<BDim> bd;
+      for (int j = 0; j < rank; ++j) {
+        if (j == d) continue;
+        bd.push_back({dims[j], first ? istrides[j] : ostrides[j], ostrides[j]});
+      }
+      P->axes.push_back(plan_axis(P.get(), dims[d], first ? istrides[d] : ostrides[d], ostrides[d],
+                                  bd, first ? B_IN : B_OUT, B_OUT));
+    }
+    if (region.empty()) {
+      // no transform: a copy (FFTA's mul! copies X into out first)
+      std::vector<BDim> bd;
+      for (int j = 1; j < rank; ++j) bd.push_back({dims[j], istrides[j], ostrides[j]});
+      LineX x;
+      make_direct(1, cutoff, dtype, &x);
+      bd.insert(bd.begin(), BDim{dims[0], istrides[0], ostrides[0]});
+      P->axes.push_back(plan_direct_axis(P.get(), 1, x, 0, 0, bd, B_IN, B_OUT));
+    }
+  }
+  if (P->scratch_elems) {
+    P->scratch0.reset(new DevBuf(P->scratch_elems * elem_bytes(dtype)));
+    bool need1 = false;
+    for (auto& ax : P->axes)
+      for (auto& p : ax.passes) need1 |= p.src == B_S1 || p.dst == B_S1;
+    if (need1) P->scratch1.reset(new DevBuf(P->scratch_elems * elem_bytes(dtype)));
+  }
+  cuda_check(cudaDeviceSynchronize(), "plan tables");
+  return P.release();
+}
+
+static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s) {
+  int dev = 0;
+  cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev != P->device) fail(FB_ERR_ARGUMENT, "plan was created on another device");
+  const int es = elem_bytes(P->dtype);
+  for (size_t ai = 0; ai < P->axes.size(); ++ai) {
+    Axis& ax = P->axes[ai];
+    int64_t nouter = 1;
+    for (auto& o : ax.outer) nouter *= o.n;
+    for (int64_t oi = 0; oi < nouter; ++oi) {
+      int64_t offi = 0, offo = 0, t = oi;
+      for (auto& o : ax.outer) {
+        const int64_t k = t % o.n;
+        t /= o.n;
+        offi += k * o.is;
+        offo += k * o.os;
+      }
+      for (size_t pi = 0; pi < ax.passes.size(); ++pi) {
+        Pass& p = ax.passes[pi];
+        LineArgs a = p.a;
+        auto resolve = [&](int id, int64_t off) -> void* {
+          switch (id) {
+            case B_IN: return (char*)in + off * es;
+            case B_OUT: return (char*)out + off * es;
+            case B_S0: return P->scratch0->p;
+            default: return P->scratch1->p;
+          }
+        };
+        // outer offsets: the source of a first pass is the user input (axis 0)
+        // or the output (later axes); both use the axis' own stride set.
+        a.in = (void*)resolve(p.src, offi);
+        a.out = resolve(p.dst, offo);
+        if (ai + 1 == P->axes.size() && pi + 1 == ax.passes.size() && P->scale != 1.0)
+          a.scale = P->scale * a.scale;
+        cuda_check(launch_line(P->dtype, p.variant, a, s), "line kernel launch");
+      }
+    }
+  }
+}
+
+static int guard(const std::function<void()>& f) {
+  try {
+    f();
+    g_last_error.clear();
+    return FB_OK;
+  } catch (FbError& e) {
+    g_last_error = e.msg;
+    return e.code;
+  } catch (std::bad_alloc&) {
+    g_last_error = "host out of memory";
+    return FB_ERR_OUT_OF_MEMORY;
+  } catch (std::exception& e) {
+    g_last_error = e.what();
+    return FB_ERR_ARGUMENT;
+  }
+}
+
+}  // namespace fb
+
+using namespace fb;
+
+extern "C" {
+
+int fb_plan_create_nd(fb_plan* plan, int dtype, int dir, int rank, const int64_t* dims,
+                      const int64_t* istrides, const int64_t* ostrides, int nregion,
+                      const int32_t* region, int64_t bluestein_cutoff, uint32_t flags) {
+  (void)flags;
+  return guard([&] {
+    if (!plan) fail(FB_ERR_ARGUMENT, "plan pointer is null");
+    *plan = nullptr;
+    if (rank < 1 || !dims || !istrides || !ostrides) fail(FB_ERR_ARGUMENT, "bad array description");
+    std::vector<int> reg;
+    for (int i = 0; i < nregion; ++i) reg.push_back(region[i] - 1);
+    *plan = create_plan(dtype, dir, rank, dims, istrides, ostrides, reg, bluestein_cutoff);
+  });
+}
+
+int fb_plan_create(fb_plan* plan, int64_t n, int dtype, int dir, int64_t batch, int64_t istride,
+                   int64_t idist, int64_t ostride, int64_t odist, int64_t bluestein_cutoff,
+                   uint32_t flags) {
+  (void)flags;
+  return guard([&] {
+    if (!plan) fail(FB_ERR_ARGUMENT, "plan pointer is null");
+    *plan = nullptr;
+    if (n <= 0) fail(FB_ERR_DIMENSION_MISMATCH, "Array length must be strictly positive");
+    if (batch < 0) fail(FB_ERR_DIMENSION_MISMATCH, "negative batch");
+    int64_t dims[2] = {n, batch}, is[2] = {istride, idist}, os[2] = {ostride, odist};
+    std::vector<int> reg{0};
+    *plan = create_plan(dtype, dir, 2, dims, is, os, reg, bluestein_cutoff);
+  });
+}
+
+int fb_plan_create_2d(fb_plan* plan, int64_t n1, int64_t n2, int dtype, int dir, int64_t batch,
+                      int64_t bluestein_cutoff, uint32_t flags) {
+  (void)flags;
+  return guard([&] {
+    if (!plan) fail(FB_ERR_ARGUMENT, "plan pointer is null");
+    *plan = nullptr;
+    if (n1 <= 0 || n2 <= 0) fail(FB_ERR_DIMENSION_MISMATCH, "Array length must be strictly positive");
+    int64_t dims[3] = {n1, n2, batch}, st[3] = {1, n1, n1 * n2};
+    std::vector<int> reg{0, 1};
+    *plan = create_plan(dtype, dir, 3, dims, st, st, reg, bluestein_cutoff);
+  });
+}
+
+int fb_plan_set_scale(fb_plan plan, double scale) {
+  return guard([&] {
+    if (!plan) fail(FB_ERR_ARGUMENT, "null plan");
+    plan->scale = scale;
+  });
+}
+
+int fb_execute(fb_plan plan, const void* in, void* out, void* stream) {
+  return guard([&] {
+    if (!plan) fail(FB_ERR_ARGUMENT, "null plan");
+    if ((!in || !out) && (plan->in_span > 0)) fail(FB_ERR_ARGUMENT, "null data pointer");
+    execute_plan(plan, in, out, (cudaStream_t)stream);
+  });
+}
+
+int fb_execute_host(fb_plan plan, const void* in, void* out, void* stream) {
+  return guard([&] {
+    if (!plan) fail(FB_ERR_ARGUMENT, "null plan");
+    if (plan->in_span == 0) return;
+    const int es = elem_bytes(plan->dtype);
+    const size_t ib = (size_t)plan->in_span * es, ob = (size_t)plan->out_span * es;
+    if (!plan->hin || plan->hin->bytes < ib) plan->hin.reset(new DevBuf(ib));
+    if (!plan->hout || plan->hout->bytes < ob) plan->hout.reset(new DevBuf(ob));
+    cudaStream_t s = (cudaStream_t)stream;
+    cuda_check(cudaMemcpyAsync(plan->hin->p, in, ib, cudaMemcpyHostToDevice, s), "copy in");
+    if (ob > ib || plan->out_span != plan->in_span) {
+      // outputs that no pass writes keep the host's values
+      cuda_check(cudaMemcpyAsync(plan->hout->p, out, ob, cudaMemcpyHostToDevice, s), "copy out init");
+    }
+    execute_plan(plan, plan->hin->p, plan->hout->p, s);
+    cuda_check(cudaMemcpyAsync(out, plan->hout->p, ob, cudaMemcpyDeviceToHost, s), "copy out");
+    cuda_check(cudaStreamSynchronize(s), "synchronize");
+  });
+}
+
+int fb_plan_size(fb_plan plan, int i, int64_t* out) {
+  return guard([&] {
+    if (!plan || !out) fail(FB_ERR_ARGUMENT, "null argument");
+    if (i < 1) fail(FB_ERR_DOMAIN, "No non-positive dimensions");
+    if (i > (int)plan->region.size())
+      *out = 1;
+    else
+      *out = plan->dims[plan->region[i - 1]];
+  });
+}
+
+int fb_plan_device_bytes(fb_plan plan, size_t* out) {
+  return guard([&] {
+    if (!plan || !out) fail(FB_ERR_ARGUMENT, "null argument");
+    size_t b = plan->table_bytes;
+    if (plan->scratch0) b += plan->scratch0->bytes;
+    if (plan->scratch1) b += plan->scratch1->bytes;
+    *out = b;
+  });
+}
+
+int fb_plan_describe(fb_plan plan, char* buf, size_t len) {
+  return guard([&] {
+    if (!plan || !buf || !len) fail(FB_ERR_ARGUMENT, "null argument");
+    std::ostringstream o;
+    o << (plan->dtype == FB_C32 ? "C32" : "C64") << (plan->dir < 0 ? " fwd" : " bwd");
+    for (auto& ax : plan->axes) {
+      o << " | n=" << ax.n << " " << ax.kind;
+      if (!ax.outer.empty()) o << " (host loop " << ax.outer.size() << " dims)";
+      for (auto& p : ax.passes) o << " " << p.what;
+    }
+    std::string s = o.str();
+    std::snprintf(buf, len, "%s", s.c_str());
+  });
+}
+
+int fb_plan_destroy(fb_plan plan) {
+  return guard([&] { delete plan; });
+}
+
+int fb_kernel_error_flag(int* value, int reset) {
+  return guard([&] {
+    if (!value) fail(FB_ERR_ARGUMENT, "null argument");
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    const DeviceTables& dt = device_tables(dev);
+    cuda_check(cudaMemcpy(value, dt.err, sizeof(int), cudaMemcpyDeviceToHost), "read flag");
+    if (reset) cuda_check(cudaMemset(dt.err, 0, sizeof(int)), "reset flag");
+  });
+}
+
+const char* fb_last_error(void) { return g_last_error.c_str(); }
+const char* fb_version(void) { return FB_VERSION; }
+
+}  // extern "C"

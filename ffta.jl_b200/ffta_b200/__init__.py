@@ -1,0 +1,427 @@
+"""ffta_b200 -- FFTA.jl's complex transform API over the sm_100a C ABI.
+
+Mirrors the plan/transform interface FFTA implements for AbstractFFTs
+(FFTA src/plan.jl):
+
+  plan_fft(x, region; BLUESTEIN_CUTOFF=73)   src/plan.jl:71-72, 77-100
+  plan_bfft(x, region; ...)                  src/plan.jl:74-75
+  p * x                                      src/plan.jl:374-384
+  mul_(y, p, x)      (Julia's mul!)          src/plan.jl:157-285
+  size(p), size(p, i)                        src/plan.jl:36-47
+  fft / bfft / ifft  (AbstractFFTs front-ends: ifft is bfft scaled by 1/n)
+
+Regions are Julia's: 1-based dimension numbers (dim d is numpy/torch axis
+d-1), an int, a tuple, a list or a range.  Arrays are numpy arrays (host) or
+torch CUDA tensors (device) of complex64/complex128; float32/float64 inputs
+are promoted to complex as AbstractFFTs does.  Every other element type raises
+ArgumentError: there is no CPU fallback.  Errors raise the Python analogues of
+FFTA's exceptions (DimensionMismatch, ArgumentError, DomainError) with FFTA's
+messages.
+"""
+from __future__ import annotations
+
+import ctypes
+from collections.abc import Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import lib
+
+__all__ = [
+    "FFT_FORWARD", "FFT_BACKWARD", "DEFAULT_BLUESTEIN_CUTOFF", "DimensionMismatch",
+    "ArgumentError", "DomainError", "CudaError", "UnsupportedError", "FFTAPlan_cx", "plan_fft",
+    "plan_bfft", "plan_ifft", "fft", "bfft", "ifft", "mul_", "size", "version",
+]
+
+FFT_FORWARD = -1  # src/callgraph.jl:1
+FFT_BACKWARD = 1
+DEFAULT_BLUESTEIN_CUTOFF = 73  # src/callgraph.jl:44
+
+
+class DimensionMismatch(Exception):
+    """Julia's DimensionMismatch."""
+
+
+class ArgumentError(Exception):
+    """Julia's ArgumentError."""
+
+
+class DomainError(Exception):
+    """Julia's DomainError."""
+
+
+class CudaError(RuntimeError):
+    """A CUDA runtime failure, or no CUDA device (there is no CPU fallback)."""
+
+
+class UnsupportedError(RuntimeError):
+    """A length this build has no kernel schedule for."""
+
+
+_STATUS = {
+    _lib.FB_ERR_DIMENSION_MISMATCH: DimensionMismatch,
+    _lib.FB_ERR_ARGUMENT: ArgumentError,
+    _lib.FB_ERR_DOMAIN: DomainError,
+    _lib.FB_ERR_CUDA: CudaError,
+    _lib.FB_ERR_UNSUPPORTED: UnsupportedError,
+    _lib.FB_ERR_OUT_OF_MEMORY: MemoryError,
+}
+
+
+def _check(rc: int) -> None:
+    if rc != _lib.FB_OK:
+        raise _STATUS.get(rc, RuntimeError)(_lib.last_error())
+
+
+def version() -> str:
+    return lib.fb_version().decode()
+
+
+# ------------------------------------------------------------------ arrays
+def _is_torch(x) -> bool:
+    t = type(x)
+    return t.__module__.startswith("torch") and t.__name__ == "Tensor"
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _complex_dtype_name(x) -> str:
+    """'c64' / 'c128' after AbstractFFTs' real -> complex promotion, else raise."""
+    if _is_torch(x):
+        torch = _torch()
+        m = {torch.complex64: "c64", torch.complex128: "c128", torch.float32: "f32",
+             torch.float64: "f64"}
+        k = m.get(x.dtype)
+    else:
+        k = {np.dtype(np.complex64): "c64", np.dtype(np.complex128): "c128",
+             np.dtype(np.float32): "f32", np.dtype(np.float64): "f64"}.get(np.asarray(x).dtype)
+    if k is None:
+        raise ArgumentError(
+            f"element type {x.dtype} is not supported: only ComplexF32/ComplexF64 (and "
+            "Float32/Float64, promoted to complex) run on the GPU, and there is no CPU fallback")
+    return {"f32": "c64", "f64": "c128"}.get(k, k)
+
+
+def _promote(x):
+    """Apply AbstractFFTs' complexfloat promotion; reject other element types."""
+    kind = _complex_dtype_name(x)
+    if _is_torch(x):
+        torch = _torch()
+        want = torch.complex64 if kind == "c64" else torch.complex128
+        return x if x.dtype == want else x.to(want)
+    x = np.asarray(x)
+    want = np.complex64 if kind == "c64" else np.complex128
+    return x if x.dtype == want else x.astype(want)
+
+
+def _shape(x):
+    return tuple(int(s) for s in x.shape)
+
+
+def _elem_strides(x):
+    """Element strides of x, or None when x needs a copy (negative/odd strides)."""
+    if _is_torch(x):
+        st = tuple(int(s) for s in x.stride())
+        return None if any(s < 0 for s in st) else st
+    item = x.itemsize
+    st = []
+    for s in x.strides:
+        if s < 0 or s % item:
+            return None
+        st.append(s // item)
+    return tuple(st)
+
+
+def _similar(x):
+    """Julia's similar(x): a new array of the same shape and element type."""
+    if _is_torch(x):
+        torch = _torch()
+        if x.is_contiguous():
+            return torch.empty_like(x, memory_format=torch.contiguous_format)
+        # keep a dense layout with the same dim order when x is dense
+        return torch.empty_like(x)
+    order = "F" if (x.flags.f_contiguous and not x.flags.c_contiguous) else "C"
+    return np.empty(x.shape, dtype=x.dtype, order=order)
+
+
+def _normalize_region(region, nd):
+    """Return (stored region object, sorted tuple) following FFTA's _sort."""
+    if region is None:
+        region = range(1, nd + 1)
+    if isinstance(region, (int, np.integer)):
+        r = int(region)
+        return r, (r,)
+    if isinstance(region, range):
+        vals = tuple(region)
+        return region if vals == tuple(sorted(vals)) else sorted(vals), tuple(sorted(vals))
+    if isinstance(region, tuple):
+        vals = tuple(int(v) for v in region)
+        return tuple(sorted(vals)), tuple(sorted(vals))
+    if isinstance(region, Sequence) or isinstance(region, np.ndarray):
+        vals = [int(v) for v in region]
+        return sorted(vals), tuple(sorted(vals))
+    raise ArgumentError(f"invalid region {region!r}")
+
+
+def _region_isvalid_nd(r, N):
+    """region_isvalid(r, N), src/plan.jl:350-359 (ND plan, ND array)."""
+    if isinstance(r, int):
+        return r == N == 1
+    return list(r) == list(range(1, N + 1))
+
+
+def _region_isvalid_md(r, M):
+    """region_isvalid(r, M, N), src/plan.jl:350-370 (M-dim plan, N-dim array)."""
+    if isinstance(r, int):
+        return M == 1
+    vals = list(r)
+    if len(vals) != M:
+        return False
+    return all(a < b for a, b in zip(vals, vals[1:]))
+
+
+# ------------------------------------------------------------------ plans
+class FFTAPlan_cx:
+    """A complex transform plan (FFTA's FFTAPlan_cx, src/plan.jl:9-20).
+
+    Holds the transform sizes and the region; the device schedules (one C plan
+    per array layout it is applied to) are created on first use and cached.
+    """
+
+    def __init__(self, sizes, region, direction, dtype_kind, cutoff, scale=1.0):
+        self._sizes = tuple(sizes)
+        self.region = region
+        self.dir = direction
+        self._kind = dtype_kind  # "c64" / "c128"
+        self.BLUESTEIN_CUTOFF = cutoff
+        self.scale = scale
+        self._cplans = {}
+
+    # -- AbstractFFTs surface
+    def size(self, i=None):
+        """Base.size(p) / Base.size(p, i) (src/plan.jl:36-47)."""
+        if i is None:
+            return self._sizes
+        i = int(i)
+        if i < 1:
+            raise DomainError(f"{i}: No non-positive dimensions")
+        if i > len(self._sizes):
+            return 1
+        return self._sizes[i - 1]
+
+    @property
+    def ndims(self):
+        return len(self._sizes)
+
+    def __mul__(self, x):
+        """p * x (src/plan.jl:374-384): allocate y = similar(x) and mul!."""
+        x = self._accept(x)
+        y = _similar(x)
+        return mul_(y, self, x)
+
+    def __matmul__(self, x):
+        return self.__mul__(x)
+
+    def __del__(self):
+        try:
+            for h in self._cplans.values():
+                lib.fb_plan_destroy(h)
+        except Exception:
+            pass
+
+    def describe(self, x) -> str:
+        """The device schedule used for arrays shaped and strided like x."""
+        x = self._accept(x)
+        h = self._cplan(x, x)
+        buf = ctypes.create_string_buffer(4096)
+        _check(lib.fb_plan_describe(h, buf, len(buf)))
+        return buf.value.decode()
+
+    def device_bytes(self, x) -> int:
+        x = self._accept(x)
+        h = self._cplan(x, x)
+        v = ctypes.c_size_t()
+        _check(lib.fb_plan_device_bytes(h, ctypes.byref(v)))
+        return int(v.value)
+
+    # -- internals
+    def _accept(self, x):
+        if not _is_torch(x):
+            x = np.asarray(x)
+        kind = _complex_dtype_name(x)
+        if kind != self._kind:
+            raise ArgumentError(
+                f"plan is for {self._kind} arrays but got {kind} (FFTA plans are typed, "
+                "src/plan.jl:9)")
+        return _promote(x)
+
+    def _regions_for(self, nd):
+        r = self.region
+        if nd == 1 and self.ndims == 1:
+            return [1]  # a 1D plan applied to a vector (src/plan.jl:157-167)
+        return [r] if isinstance(r, int) else list(r)
+
+    def _cplan(self, y, x):
+        xs, ys = _elem_strides(x), _elem_strides(y)
+        key = (_shape(x), xs, ys)
+        h = self._cplans.get(key)
+        if h is not None:
+            return h
+        nd = x.ndim
+        dims = (ctypes.c_int64 * nd)(*_shape(x))
+        ist = (ctypes.c_int64 * nd)(*xs)
+        ost = (ctypes.c_int64 * nd)(*ys)
+        reg = self._regions_for(nd)
+        creg = (ctypes.c_int32 * max(1, len(reg)))(*reg)
+        handle = ctypes.c_void_p()
+        dt = _lib.FB_C32 if self._kind == "c64" else _lib.FB_C64
+        _check(lib.fb_plan_create_nd(ctypes.byref(handle), dt, self.dir, nd, dims, ist, ost,
+                                     len(reg), creg, int(self.BLUESTEIN_CUTOFF), 0))
+        if self.scale != 1.0:
+            _check(lib.fb_plan_set_scale(handle, float(self.scale)))
+        self._cplans[key] = handle
+        return handle
+
+
+def _make_plan(x, region, direction, cutoff, scale_inverse=False):
+    if not _is_torch(x):
+        x = np.asarray(x)
+    kind = _complex_dtype_name(x)
+    nd = x.ndim
+    stored, srt = _normalize_region(region, nd)
+    shape = _shape(x)
+    sizes = []
+    for r in srt:
+        if r < 1 or r > nd:
+            # FFTA reads size(x, R) which is 1 beyond ndims; CallGraph(1) is fine,
+            # and mul! later rejects the region.
+            sizes.append(1 if r > nd else 0)
+        else:
+            sizes.append(shape[r - 1])
+    for s in sizes:
+        if s <= 0:
+            raise DimensionMismatch("Array length must be strictly positive")
+    scale = 1.0
+    if scale_inverse:
+        scale = 1.0 / float(np.prod(sizes))
+    return FFTAPlan_cx(sizes, stored, direction, kind, int(cutoff), scale)
+
+
+def plan_fft(x, region=None, *, BLUESTEIN_CUTOFF=DEFAULT_BLUESTEIN_CUTOFF, **_kwargs):
+    """AbstractFFTs.plan_fft (FFTA src/plan.jl:71-72)."""
+    return _make_plan(x, region, FFT_FORWARD, BLUESTEIN_CUTOFF)
+
+
+def plan_bfft(x, region=None, *, BLUESTEIN_CUTOFF=DEFAULT_BLUESTEIN_CUTOFF, **_kwargs):
+    """AbstractFFTs.plan_bfft (FFTA src/plan.jl:74-75): unnormalised inverse."""
+    return _make_plan(x, region, FFT_BACKWARD, BLUESTEIN_CUTOFF)
+
+
+def plan_ifft(x, region=None, *, BLUESTEIN_CUTOFF=DEFAULT_BLUESTEIN_CUTOFF, **_kwargs):
+    """AbstractFFTs.plan_ifft: plan_bfft scaled by 1/prod(sizes), fused in-kernel."""
+    return _make_plan(x, region, FFT_BACKWARD, BLUESTEIN_CUTOFF, scale_inverse=True)
+
+
+def size(p: FFTAPlan_cx, i=None):
+    return p.size(i)
+
+
+def mul_(y, p: FFTAPlan_cx, x):
+    """LinearAlgebra.mul!(y, p, x) with FFTA's argument checks (src/plan.jl:157-285)."""
+    x = p._accept(x)
+    if _is_torch(y) != _is_torch(x):
+        raise ArgumentError("input and output must both be host arrays or both device tensors")
+    if not _is_torch(y):
+        y = np.asarray(y)
+    if _complex_dtype_name(y) != p._kind or (not _is_torch(y) and y.dtype != x.dtype):
+        raise ArgumentError("output element type must match the plan")
+    N, M = x.ndim, p.ndims
+    r = p.region
+    xs, ys = _shape(x), _shape(y)
+    if M == 1:
+        # 1D plan: vector (src/plan.jl:157-167) or N-D array (src/plan.jl:170-192)
+        if xs != ys:
+            raise DimensionMismatch(f"input array has axes {xs}, but output array has axes {ys}")
+        R1 = r if isinstance(r, int) else (list(r)[0] if len(list(r)) == 1 else None)
+        if R1 is None:
+            raise DimensionMismatch("Region is invalid.")
+        if N == 1:
+            if p.size() != xs:
+                raise DimensionMismatch(f"plan has axes {p.size()}, but input array has axes {xs}")
+        else:
+            if R1 < 1 or R1 > N:
+                raise DimensionMismatch("Plan region is outside array dimensions.")
+            if p.size(1) != xs[R1 - 1]:
+                raise DimensionMismatch(
+                    f"plan has size {p.size(1)}, but input array has size {xs[R1 - 1]} along "
+                    f"region {R1}")
+    elif M == N:
+        # ND plan, ND array (src/plan.jl:210-222)
+        if xs != ys:
+            raise DimensionMismatch(f"input array has axes {xs}, but output array has axes {ys}")
+        if p.size() != xs:
+            raise DimensionMismatch(f"plan has size {p.size()}, but input array has size {xs}")
+        if not _region_isvalid_nd(r, N):
+            raise DimensionMismatch("Plan region is outside array dimensions.")
+    else:
+        # M-dim plan on an N-dim array (src/plan.jl:260-272)
+        if xs != ys:
+            raise DimensionMismatch(f"input array has axes {xs}, but output array has axes {ys}")
+        if not _region_isvalid_md(r, M):
+            raise DimensionMismatch("Region is invalid.")
+        vals = list(r)
+        if M > N or vals[0] < 1 or vals[-1] > N:
+            raise DimensionMismatch("Plan region is outside array dimensions.")
+        for k, d in enumerate(vals):
+            if p.size(k + 1) != xs[d - 1]:
+                raise DimensionMismatch(
+                    f"plan has size {p.size()}, but input array has size {xs}")
+    if x.size == 0:
+        return y
+    # The C plan needs element strides; copy views it cannot address.
+    if _elem_strides(x) is None:
+        x = x.contiguous() if _is_torch(x) else np.ascontiguousarray(x)
+    y_target = y
+    if _elem_strides(y) is None:
+        y = _similar(y)
+    h = p._cplan(y, x)
+    if _is_torch(x):
+        torch = _torch()
+        if not x.is_cuda or not y.is_cuda:
+            raise ArgumentError("torch tensors must live on a CUDA device")
+        stream = torch.cuda.current_stream(x.device).cuda_stream
+        with torch.cuda.device(x.device):
+            _check(lib.fb_execute(h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(y.data_ptr()),
+                                  ctypes.c_void_p(stream)))
+    else:
+        _check(lib.fb_execute_host(h, ctypes.c_void_p(x.ctypes.data), ctypes.c_void_p(y.ctypes.data),
+                                   None))
+    if y is not y_target:
+        y_target[...] = y
+        y = y_target
+    return y
+
+
+def _apply(planner, x, region, **kw):
+    x = _promote(x if _is_torch(x) else np.asarray(x))
+    p = planner(x, region, **kw)
+    return p * x
+
+
+def fft(x, region=None, **kw):
+    """AbstractFFTs fft(x, region) -> plan_fft(x, region) * x."""
+    return _apply(plan_fft, x, region, **kw)
+
+
+def bfft(x, region=None, **kw):
+    """AbstractFFTs bfft(x, region) -> plan_bfft(x, region) * x (unnormalised)."""
+    return _apply(plan_bfft, x, region, **kw)
+
+
+def ifft(x, region=None, **kw):
+    """AbstractFFTs ifft: bfft scaled by 1/prod(sizes along region)."""
+    return _apply(plan_ifft, x, region, **kw)

@@ -1,0 +1,119 @@
+/* fftab200.h -- C ABI of libfftab200.so, the sm_100a transform library that
+ * stands in for FFTA.jl's complex transform path.
+ *
+ * FFTA.jl is pure Julia; its entry points are AbstractFFTs methods.  Each
+ * function below names the FFTA method it replaces (file:line inside the
+ * FFTA.jl repository).  A Julia binding calls these with `ccall` (see
+ * INTEGRATION.md); the Python package ffta_b200 calls them with ctypes.
+ *
+ * Conventions
+ *  - Complex data are interleaved (re, im) pairs: ComplexF32 = 2 x float,
+ *    ComplexF64 = 2 x double, the memory layout of Julia's Complex{T}.
+ *  - Strides and distances are in elements, not bytes.
+ *  - `dir` is FB_FORWARD (-1, FFTA's FFT_FORWARD) or FB_BACKWARD (+1,
+ *    FFT_BACKWARD, unnormalised), FFTA src/callgraph.jl:1.
+ *  - Every function returns an FB_* status; fb_last_error() gives the
+ *    message of the last failure on the calling thread.  Statuses map to the
+ *    Julia exception FFTA throws in the same situation.
+ *  - There is no CPU fallback: without a CUDA device every plan call fails
+ *    with FB_ERR_CUDA.
+ */
+#ifndef FFTAB200_H
+#define FFTAB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fb_plan_s* fb_plan;
+
+enum {
+  FB_OK = 0,
+  FB_ERR_DIMENSION_MISMATCH = 1, /* Julia DimensionMismatch */
+  FB_ERR_ARGUMENT = 2,           /* Julia ArgumentError */
+  FB_ERR_DOMAIN = 3,             /* Julia DomainError */
+  FB_ERR_CUDA = 4,               /* CUDA runtime failure, or no device */
+  FB_ERR_UNSUPPORTED = 5,        /* a length this build has no schedule for */
+  FB_ERR_OUT_OF_MEMORY = 6
+};
+
+enum { FB_C32 = 0, FB_C64 = 1 };          /* ComplexF32, ComplexF64 */
+enum { FB_FORWARD = -1, FB_BACKWARD = 1 };
+enum { FB_DEFAULT_BLUESTEIN_CUTOFF = 73 }; /* src/callgraph.jl:44 */
+
+/* Batched 1-D plan: `batch` transforms of length n; element j of transform b
+ * is read at in[b*idist + j*istride] and written at out[b*odist + j*ostride].
+ * Replaces plan_fft/plan_bfft with a one-dimensional region
+ * (src/plan.jl:71-87) together with the 1-D executors mul! for a vector
+ * (src/plan.jl:157-167) and for the columns of an array (src/plan.jl:170-207).
+ * n <= 0 gives FB_ERR_DIMENSION_MISMATCH ("Array length must be strictly
+ * positive", src/callgraph.jl:83-85).  Primes >= bluestein_cutoff go through
+ * Bluestein (src/callgraph.jl:95-100). */
+int fb_plan_create(fb_plan* plan, int64_t n, int dtype, int dir, int64_t batch, int64_t istride,
+                   int64_t idist, int64_t ostride, int64_t odist, int64_t bluestein_cutoff,
+                   uint32_t flags);
+
+/* 2-D plan over `batch` contiguous column-major n1 x n2 matrices (dim 1
+ * contiguous).  Replaces plan_fft(X) with region 1:2 (src/plan.jl:88-92) and
+ * the N-D executor mul! (src/plan.jl:210-257, fft_along_dim! :327-348). */
+int fb_plan_create_2d(fb_plan* plan, int64_t n1, int64_t n2, int dtype, int dir, int64_t batch,
+                      int64_t bluestein_cutoff, uint32_t flags);
+
+/* General plan over a strided array of `rank` dims: dims[d] elements with
+ * element strides istrides[d] (input) and ostrides[d] (output), transformed
+ * along the 1-based dims listed in `region` (strictly ascending).  Replaces
+ * plan_fft/plan_bfft for any region (src/plan.jl:77-100) and the executors
+ * for 1-D, N-D and M<N plans (src/plan.jl:170-325).  A region that is not
+ * strictly ascending gives "Region is invalid." and one outside 1..rank
+ * "Plan region is outside array dimensions." (src/plan.jl:268-271), both
+ * FB_ERR_DIMENSION_MISMATCH. */
+int fb_plan_create_nd(fb_plan* plan, int dtype, int dir, int rank, const int64_t* dims,
+                      const int64_t* istrides, const int64_t* ostrides, int nregion,
+                      const int32_t* region, int64_t bluestein_cutoff, uint32_t flags);
+
+/* Multiply every output by `scale` (fused into the last kernel).  ifft is
+ * bfft scaled by 1/prod(n) (AbstractFFTs ScaledPlan). */
+int fb_plan_set_scale(fb_plan plan, double scale);
+
+/* Run the plan on device pointers, enqueued on `stream` (a cudaStream_t; NULL
+ * is the legacy default stream).  Input and output may be the same buffer.
+ * Replaces LinearAlgebra.mul!(y, p, x) (src/plan.jl:157,170,210,260). */
+int fb_execute(fb_plan plan, const void* in, void* out, void* stream);
+
+/* Run the plan on host arrays: copies in, transforms, copies out, and returns
+ * when `out` holds the result.  Pinned host memory gives full copy speed.
+ * Replaces Base.:*(p, x) on a CPU array (src/plan.jl:374-384). */
+int fb_execute_host(fb_plan plan, const void* in, void* out, void* stream);
+
+/* Base.size(p, i) (src/plan.jl:36-47): the transform length along the i-th
+ * region entry, 1 past the last one, FB_ERR_DOMAIN for i < 1. */
+int fb_plan_size(fb_plan plan, int i, int64_t* out);
+
+/* Device bytes held by the plan (tables and scratch). */
+int fb_plan_device_bytes(fb_plan plan, size_t* out);
+
+/* Human-readable schedule (kernel passes, radices, launch shapes). */
+int fb_plan_describe(fb_plan plan, char* buf, size_t len);
+
+int fb_plan_destroy(fb_plan plan);
+
+/* Diagnostic: the current device's kernel error flag (0, or a radix that a
+ * stage program named without a butterfly for it), optionally reset.  No
+ * FFTA counterpart: FFTA raises ArgumentError("kernel not implemented")
+ * for an unknown node type (src/algos.jl:31). */
+int fb_kernel_error_flag(int* value, int reset);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* fb_last_error(void);
+
+/* Library version string. */
+const char* fb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FFTAB200_H */
