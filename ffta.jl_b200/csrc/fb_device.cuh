@@ -74,6 +74,12 @@ template <> struct K<float> {
   static constexpr float c52 = -0.80901699437494742410f; // cos(4pi/5)
   static constexpr float s51 = 0.95105651629515357212f;  // sin(2pi/5)
   static constexpr float s52 = 0.58778525229247312917f;  // sin(4pi/5)
+  static constexpr float c91 = 0.76604444311897803520f;  // cos(2pi/9)
+  static constexpr float s91 = 0.64278760968653932632f;  // sin(2pi/9)
+  static constexpr float c92 = 0.17364817766693034885f;  // cos(4pi/9)
+  static constexpr float s92 = 0.98480775301220805936f;  // sin(4pi/9)
+  static constexpr float c94 = -0.93969262078590838405f; // cos(8pi/9)
+  static constexpr float s94 = 0.34202014332566873304f;  // sin(8pi/9)
 };
 template <> struct K<double> {
   static constexpr double r2 = 0.70710678118654752440;
@@ -84,6 +90,12 @@ template <> struct K<double> {
   static constexpr double c52 = -0.80901699437494742410;
   static constexpr double s51 = 0.95105651629515357212;
   static constexpr double s52 = 0.58778525229247312917;
+  static constexpr double c91 = 0.76604444311897803520;
+  static constexpr double s91 = 0.64278760968653932632;
+  static constexpr double c92 = 0.17364817766693034885;
+  static constexpr double s92 = 0.98480775301220805936;
+  static constexpr double c94 = -0.93969262078590838405;
+  static constexpr double s94 = 0.34202014332566873304;
 };
 
 // -------------------------------------------------------- butterflies
@@ -180,6 +192,29 @@ template <typename R, int DIR> __device__ __forceinline__ void dft3(cplx<R>* v) 
   v[0] = cadd<R>(v[0], t);
   v[1] = cadd<R>(m, j);
   v[2] = csub<R>(m, j);
+}
+
+// 9 = 3 x 3: n = 3 n1 + n2, k = k1 + 3 k2, inner twiddles w9^(n2 k1).
+template <typename R, int DIR> __device__ __forceinline__ void dft9(cplx<R>* v) {
+  cplx<R> b[3][3];
+#pragma unroll
+  for (int n2 = 0; n2 < 3; ++n2) {
+    cplx<R> t[3] = {v[n2], v[3 + n2], v[6 + n2]};
+    dft3<R, DIR>(t);
+#pragma unroll
+    for (int k1 = 0; k1 < 3; ++k1) b[n2][k1] = t[k1];
+  }
+  b[1][1] = mulcs<R, DIR>(b[1][1], K<R>::c91, K<R>::s91);  // w9^1
+  b[1][2] = mulcs<R, DIR>(b[1][2], K<R>::c92, K<R>::s92);  // w9^2
+  b[2][1] = mulcs<R, DIR>(b[2][1], K<R>::c92, K<R>::s92);  // w9^2
+  b[2][2] = mulcs<R, DIR>(b[2][2], K<R>::c94, K<R>::s94);  // w9^4
+#pragma unroll
+  for (int k1 = 0; k1 < 3; ++k1) {
+    cplx<R> t[3] = {b[0][k1], b[1][k1], b[2][k1]};
+    dft3<R, DIR>(t);
+#pragma unroll
+    for (int k2 = 0; k2 < 3; ++k2) v[k1 + 3 * k2] = t[k2];
+  }
 }
 
 template <typename R, int DIR> __device__ __forceinline__ void dft5(cplx<R>* v) {

@@ -59,6 +59,30 @@ struct LineArgs {
                         // this kernel has no butterfly for (never traps)
 };
 
+// Arguments of the specialised direct-I/O kernel (fb_fast.cuh): `nlines`
+// contiguous lines of length L, line l at in + l*idist / out + l*odist.
+struct FastArgs {
+  const void* in;
+  void* out;
+  int64_t nlines, idist, odist;
+  const void* tw;
+  const void* prime_cs;
+  double scale;
+  int G;
+};
+
+// One specialised length: its radix program, threads per line, launcher and
+// padded shared-memory elements per line.
+struct FastFn {
+  int L, T, nst;
+  int radix[8];
+  cudaError_t (*launch)(int dir, const FastArgs&, cudaStream_t);
+  cudaError_t (*launch_staged)(const LineArgs&, cudaStream_t);
+  size_t lpad;
+};
+const FastFn* fast_table_f32(int* count);
+const FastFn* fast_table_f64(int* count);
+
 // Offsets (in (cos,sin) pairs) of each odd prime's table inside prime_cs.
 int prime_table_offset(int p);
 int prime_table_total();

@@ -64,6 +64,8 @@ __device__ __forceinline__ void butterfly(cplx<R>* v, const R* pcs) {
     dft5<R, DIR>(v);
   } else if constexpr (RAD == 8) {
     dft8<R, DIR>(v);
+  } else if constexpr (RAD == 9) {
+    dft9<R, DIR>(v);
   } else if constexpr (RAD == 16) {
     dft16<R, DIR>(v);
   } else {
@@ -76,7 +78,7 @@ __device__ __forceinline__ void butterfly(cplx<R>* v, const R* pcs) {
 // Butterfly j (k = j mod Ns) reads x[j + r*L/RAD], twiddles input r by
 // w_{Ns*RAD}^(r k), and writes y[(j-k)*RAD + k + r*Ns].
 template <typename R, int RAD, int DIR, int CAP>
-__device__ __forceinline__ void stage(cplx<R>* buf, int L, int Ns, const cplx<R>* __restrict__ tw,
+__device__ __noinline__ void stage(cplx<R>* buf, int L, int Ns, const cplx<R>* __restrict__ tw,
                                       const R* pcs, int u, int T) {
   constexpr int UM = (RAD >= CAP) ? 1 : CAP / RAD;
   const int nb = L / RAD;
@@ -110,7 +112,7 @@ __device__ __forceinline__ void stage(cplx<R>* buf, int L, int Ns, const cplx<R>
 }
 
 template <typename R, int DIR, int CAP, bool BIG>
-__device__ __noinline__ void run_prog(cplx<R>* buf, const StageProg& p, const R* pcs, int u,
+__device__ __forceinline__ void run_prog(cplx<R>* buf, const StageProg& p, const R* pcs, int u,
                                          int T, int* err) {
   const cplx<R>* twb = (const cplx<R>*)p.tw;
   int Ns = 1;
@@ -125,6 +127,7 @@ __device__ __noinline__ void run_prog(cplx<R>* buf, const StageProg& p, const R*
       case 5: stage<R, 5, DIR, CAP>(buf, L, Ns, tw, pcs, u, T); break;
       case 7: stage<R, 7, DIR, CAP>(buf, L, Ns, tw, pcs, u, T); break;
       case 8: stage<R, 8, DIR, CAP>(buf, L, Ns, tw, pcs, u, T); break;
+      case 9: stage<R, 9, DIR, CAP>(buf, L, Ns, tw, pcs, u, T); break;
       case 11: stage<R, 11, DIR, CAP>(buf, L, Ns, tw, pcs, u, T); break;
       case 13: stage<R, 13, DIR, CAP>(buf, L, Ns, tw, pcs, u, T); break;
       case 16: stage<R, 16, DIR, CAP>(buf, L, Ns, tw, pcs, u, T); break;
@@ -267,20 +270,22 @@ __global__ void __launch_bounds__(512) line_kernel(const LineArgs a) {
   __syncthreads();
   C* buf = sm + g * a.Lpad;
   const R* pcs = (const R*)a.prime_cs;
-  if (a.dir1 < 0)
-    run_prog<R, -1, CAP, BIG>(buf, a.prog, pcs, u, T, a.err);
-  else
-    run_prog<R, 1, CAP, BIG>(buf, a.prog, pcs, u, T, a.err);
-  if (a.mid) {
-    const C* __restrict__ mid = (const C*)a.mid;
-    const int64_t l0 = lb[2 * G + g];
-    for (int k = u; k < a.prog.L; k += T)
-      buf[padi(k)] = cmul<R>(buf[padi(k)], __ldg(mid + l0 * a.mid_ls + (int64_t)k * a.mid_es));
-    __syncthreads();
-    if (a.dir2 < 0)
+  // One program, or (Bluestein) program -> pointwise multiply -> program in
+  // the other direction.  The loop keeps one inlined copy per direction.
+  const int npass = a.mid ? 2 : 1;
+#pragma unroll 1
+  for (int ps = 0; ps < npass; ++ps) {
+    if ((ps == 0 ? a.dir1 : a.dir2) < 0)
       run_prog<R, -1, CAP, BIG>(buf, a.prog, pcs, u, T, a.err);
     else
       run_prog<R, 1, CAP, BIG>(buf, a.prog, pcs, u, T, a.err);
+    if (ps == 0 && a.mid) {
+      const C* __restrict__ mid = (const C*)a.mid;
+      const int64_t l0 = lb[2 * G + g];
+      for (int k = u; k < a.prog.L; k += T)
+        buf[padi(k)] = cmul<R>(buf[padi(k)], __ldg(mid + l0 * a.mid_ls + (int64_t)k * a.mid_es));
+      __syncthreads();
+    }
   }
   store_lines<R>(a, sm, lb, line0, tid, nthr);
 }

@@ -133,7 +133,8 @@ static int um_for(int R, int cap) { return R >= cap ? 1 : cap / R; }
 
 // Radix program for a length whose prime factors are all <= FB_MAX_PRIME:
 // powers of two as radix 16 with an 8, 4 or 2 (8*4 in place of 16*2), then
-// threes, fives and the odd primes in ascending order.
+// powers of three as radix 9 with a final 3, then fives and the odd primes
+// in ascending order.  The program depends on the length alone.
 static std::vector<int> radix_program(int64_t L) {
   std::vector<int> r;
   int a = 0;
@@ -152,6 +153,13 @@ static std::vector<int> radix_program(int64_t L) {
     if (rem == 2) r.push_back(4);
     if (rem == 3) r.push_back(8);
   }
+  int b = 0;
+  while (L % 3 == 0) {
+    L /= 3;
+    ++b;
+  }
+  for (int i = 0; i < b / 2; ++i) r.push_back(9);
+  if (b % 2) r.push_back(3);
   for (auto& pe : factorize(L))
     for (int i = 0; i < pe.second; ++i) r.push_back((int)pe.first);
   return r;
@@ -244,7 +252,24 @@ struct Pass {
   int variant = 0;
   int src = B_IN, dst = B_OUT;
   std::string what;
+  const FastFn* fast = nullptr;    // specialised direct-I/O kernel, if any
+  FastArgs fa;
+  const FastFn* staged = nullptr;  // specialised stage program with generic I/O
 };
+
+// The specialised kernel for a radix program, if one is compiled.
+static const FastFn* find_fast(int dtype, int L, const std::vector<int>& radices) {
+  int cnt = 0;
+  const FastFn* t = dtype == FB_C32 ? fast_table_f32(&cnt) : fast_table_f64(&cnt);
+  for (int i = 0; i < cnt; ++i) {
+    if (t[i].L != L || t[i].nst != (int)radices.size()) continue;
+    bool same = true;
+    for (int s = 0; s < t[i].nst; ++s) same &= t[i].radix[s] == radices[s];
+    if (same) return &t[i];
+  }
+  return nullptr;
+}
+
 
 struct BDim {
   int64_t n, is, os;
@@ -261,6 +286,7 @@ struct Axis {
 
 struct fb_plan_s {
   int dtype = 0, dir = -1, device = 0;
+  uint32_t flags = 0;  // bit 0: generic kernels only (no specialised lengths)
   int64_t cutoff = 73;
   double scale = 1.0;
   int rank = 0;
@@ -277,6 +303,21 @@ struct fb_plan_s {
 };
 
 namespace fb {
+
+static int pick_G(const fb_plan_s* P, int L, int T, int Lpad, bool elem_major, int64_t nlines);
+
+// Switch a generic pass to the compile-time stage program of its length when
+// one is compiled (same arithmetic, no runtime radix dispatch).
+static void use_staged(const fb_plan_s* P, Pass& p, const std::vector<int>& radices) {
+  if (P->flags & 1) return;
+  const FastFn* ff = find_fast(P->dtype, p.a.prog.L, radices);
+  if (!ff || (int)ff->lpad != p.a.Lpad) return;
+  p.staged = ff;
+  p.a.T = ff->T;
+  const bool em = p.a.ld.mode == 1 || p.a.st.mode == 1;
+  p.a.G = pick_G(P, p.a.prog.L, ff->T, p.a.Lpad, em, p.a.nlines);
+  p.what += "[staged T=" + std::to_string(ff->T) + " G=" + std::to_string(p.a.G) + "]";
+}
 
 static void* alloc_table(fb_plan_s* P, size_t bytes) {
   P->bufs.emplace_back(new DevBuf(bytes));
@@ -319,7 +360,8 @@ static void fill_prog(fb_plan_s* P, LineX& x, StageProg* prog) {
 
 static fb_plan_s* create_plan(int dtype, int dir, int rank, const int64_t* dims,
                               const int64_t* istrides, const int64_t* ostrides,
-                              const std::vector<int>& region, int64_t cutoff);
+                              const std::vector<int>& region, int64_t cutoff,
+                              uint32_t flags = 0);
 static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s);
 
 // Chirp spectrum FFT_M(b_ext), forward, computed in FP64 by a C64 plan and
@@ -510,11 +552,39 @@ static Axis plan_direct_axis(fb_plan_s* P, int64_t n, LineX& x, int64_t is, int6
   p.a.st.mode = st_em ? 1 : 0;
   p.a.G = pick_G(P, x.L, x.T, p.a.Lpad, ld_em || st_em, nl);
   ax.kind = x.kind == 0 ? "DIRECT" : "BLUE1";
+  // Contiguous lines at one batch stride: the specialised direct-I/O kernel.
+  const FastFn* ff = nullptr;
+  if (x.kind == 0 && is == 1 && os == 1 && inner.size() <= 1 && !(P->flags & 1))
+    ff = find_fast(P->dtype, x.L, x.radices);
+  if (ff) {
+    p.fast = ff;
+    memset(&p.fa, 0, sizeof(p.fa));
+    p.fa.nlines = nl;
+    p.fa.idist = level_is(inner, 0);
+    p.fa.odist = level_os(inner, 0);
+    p.fa.tw = p.a.prog.tw;
+    p.fa.prime_cs = p.a.prime_cs;
+    p.fa.scale = 1.0;
+    const int es = elem_bytes(P->dtype);
+    int G = std::max(1, 256 / ff->T);
+    G = std::min(G, std::max(1, line_max_threads() / ff->T));
+    while (G > 1 && (size_t)G * ff->lpad * es > 100 * 1024) G /= 2;
+    while (G > 1 && G / 2 >= nl) G /= 2;
+    p.fa.G = G;
+    std::ostringstream w;
+    w << "FAST(L=" << x.L << " radices=";
+    for (size_t i = 0; i < x.radices.size(); ++i) w << (i ? "x" : "") << x.radices[i];
+    w << " T=" << ff->T << " G=" << G << ")";
+    p.what = w.str();
+    ax.passes.push_back(p);
+    return ax;
+  }
   std::ostringstream w;
   w << ax.kind << "(L=" << x.L << " radices=";
   for (size_t i = 0; i < x.radices.size(); ++i) w << (i ? "x" : "") << x.radices[i];
   w << " T=" << x.T << " G=" << p.a.G << " var=" << x.variant << ")";
   p.what = w.str();
+  use_staged(P, p, x.radices);
   ax.passes.push_back(p);
   return ax;
 }
@@ -569,6 +639,8 @@ static Axis plan_four_axis(fb_plan_s* P, int64_t N, int64_t N1, int64_t N2, Line
      << " G=" << p2.a.G << ")";
   p1.what = w1.str();
   p2.what = w2.str();
+  use_staged(P, p1, x1.radices);
+  use_staged(P, p2, x2.radices);
   ax.passes.push_back(p1);
   ax.passes.push_back(p2);
   return ax;
@@ -661,6 +733,9 @@ static Axis plan_blue3_axis(fb_plan_s* P, int64_t N, int64_t is, int64_t os,
   p1.what = w.str() + ".1";
   p2.what = w.str() + ".2";
   p3.what = w.str() + ".3";
+  use_staged(P, p1, x1.radices);
+  use_staged(P, p2, x2.radices);
+  use_staged(P, p3, x1.radices);
   ax.passes.push_back(p1);
   ax.passes.push_back(p2);
   ax.passes.push_back(p3);
@@ -704,7 +779,7 @@ static Axis plan_axis(fb_plan_s* P, int64_t n, int64_t is, int64_t os, std::vect
 
 static fb_plan_s* create_plan(int dtype, int dir, int rank, const int64_t* dims,
                               const int64_t* istrides, const int64_t* ostrides,
-                              const std::vector<int>& region, int64_t cutoff) {
+                              const std::vector<int>& region, int64_t cutoff, uint32_t flags) {
   if (dtype != FB_C32 && dtype != FB_C64)
     fail(FB_ERR_ARGUMENT, "element type must be ComplexF32 or ComplexF64");
   if (dir != FB_FORWARD && dir != FB_BACKWARD) fail(FB_ERR_ARGUMENT, "direction must be -1 or +1");
@@ -727,6 +802,7 @@ static fb_plan_s* create_plan(int dtype, int dir, int rank, const int64_t* dims,
   P->dtype = dtype;
   P->dir = dir;
   P->cutoff = cutoff;
+  P->flags = flags;
   P->rank = rank;
   P->dims.assign(dims, dims + rank);
   P->istrides.assign(istrides, istrides + rank);
@@ -814,8 +890,20 @@ static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s
         // or the output (later axes); both use the axis' own stride set.
         a.in = (void*)resolve(p.src, offi);
         a.out = resolve(p.dst, offo);
-        if (ai + 1 == P->axes.size() && pi + 1 == ax.passes.size() && P->scale != 1.0)
-          a.scale = P->scale * a.scale;
+        const bool last = ai + 1 == P->axes.size() && pi + 1 == ax.passes.size();
+        if (p.fast) {
+          FastArgs fa = p.fa;
+          fa.in = a.in;
+          fa.out = a.out;
+          if (last) fa.scale = P->scale;
+          cuda_check(p.fast->launch(P->dir, fa, s), "fast kernel launch");
+          continue;
+        }
+        if (last && P->scale != 1.0) a.scale = P->scale * a.scale;
+        if (p.staged) {
+          cuda_check(p.staged->launch_staged(a, s), "staged kernel launch");
+          continue;
+        }
         cuda_check(launch_line(P->dtype, p.variant, a, s), "line kernel launch");
       }
     }
@@ -848,21 +936,19 @@ extern "C" {
 int fb_plan_create_nd(fb_plan* plan, int dtype, int dir, int rank, const int64_t* dims,
                       const int64_t* istrides, const int64_t* ostrides, int nregion,
                       const int32_t* region, int64_t bluestein_cutoff, uint32_t flags) {
-  (void)flags;
   return guard([&] {
     if (!plan) fail(FB_ERR_ARGUMENT, "plan pointer is null");
     *plan = nullptr;
     if (rank < 1 || !dims || !istrides || !ostrides) fail(FB_ERR_ARGUMENT, "bad array description");
     std::vector<int> reg;
     for (int i = 0; i < nregion; ++i) reg.push_back(region[i] - 1);
-    *plan = create_plan(dtype, dir, rank, dims, istrides, ostrides, reg, bluestein_cutoff);
+    *plan = create_plan(dtype, dir, rank, dims, istrides, ostrides, reg, bluestein_cutoff, flags);
   });
 }
 
 int fb_plan_create(fb_plan* plan, int64_t n, int dtype, int dir, int64_t batch, int64_t istride,
                    int64_t idist, int64_t ostride, int64_t odist, int64_t bluestein_cutoff,
                    uint32_t flags) {
-  (void)flags;
   return guard([&] {
     if (!plan) fail(FB_ERR_ARGUMENT, "plan pointer is null");
     *plan = nullptr;
@@ -870,20 +956,19 @@ int fb_plan_create(fb_plan* plan, int64_t n, int dtype, int dir, int64_t batch, 
     if (batch < 0) fail(FB_ERR_DIMENSION_MISMATCH, "negative batch");
     int64_t dims[2] = {n, batch}, is[2] = {istride, idist}, os[2] = {ostride, odist};
     std::vector<int> reg{0};
-    *plan = create_plan(dtype, dir, 2, dims, is, os, reg, bluestein_cutoff);
+    *plan = create_plan(dtype, dir, 2, dims, is, os, reg, bluestein_cutoff, flags);
   });
 }
 
 int fb_plan_create_2d(fb_plan* plan, int64_t n1, int64_t n2, int dtype, int dir, int64_t batch,
                       int64_t bluestein_cutoff, uint32_t flags) {
-  (void)flags;
   return guard([&] {
     if (!plan) fail(FB_ERR_ARGUMENT, "plan pointer is null");
     *plan = nullptr;
     if (n1 <= 0 || n2 <= 0) fail(FB_ERR_DIMENSION_MISMATCH, "Array length must be strictly positive");
     int64_t dims[3] = {n1, n2, batch}, st[3] = {1, n1, n1 * n2};
     std::vector<int> reg{0, 1};
-    *plan = create_plan(dtype, dir, 3, dims, st, st, reg, bluestein_cutoff);
+    *plan = create_plan(dtype, dir, 3, dims, st, st, reg, bluestein_cutoff, flags);
   });
 }
 

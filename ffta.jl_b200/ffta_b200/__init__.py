@@ -192,7 +192,8 @@ class FFTAPlan_cx:
     per array layout it is applied to) are created on first use and cached.
     """
 
-    def __init__(self, sizes, region, direction, dtype_kind, cutoff, scale=1.0):
+    def __init__(self, sizes, region, direction, dtype_kind, cutoff, scale=1.0, flags=0):
+        self._flags = int(flags)
         self._sizes = tuple(sizes)
         self.region = region
         self.dir = direction
@@ -280,14 +281,14 @@ class FFTAPlan_cx:
         handle = ctypes.c_void_p()
         dt = _lib.FB_C32 if self._kind == "c64" else _lib.FB_C64
         _check(lib.fb_plan_create_nd(ctypes.byref(handle), dt, self.dir, nd, dims, ist, ost,
-                                     len(reg), creg, int(self.BLUESTEIN_CUTOFF), 0))
+                                     len(reg), creg, int(self.BLUESTEIN_CUTOFF), self._flags))
         if self.scale != 1.0:
             _check(lib.fb_plan_set_scale(handle, float(self.scale)))
         self._cplans[key] = handle
         return handle
 
 
-def _make_plan(x, region, direction, cutoff, scale_inverse=False):
+def _make_plan(x, region, direction, cutoff, scale_inverse=False, flags=0):
     if not _is_torch(x):
         x = np.asarray(x)
     kind = _complex_dtype_name(x)
@@ -308,22 +309,26 @@ def _make_plan(x, region, direction, cutoff, scale_inverse=False):
     scale = 1.0
     if scale_inverse:
         scale = 1.0 / float(np.prod(sizes))
-    return FFTAPlan_cx(sizes, stored, direction, kind, int(cutoff), scale)
+    return FFTAPlan_cx(sizes, stored, direction, kind, int(cutoff), scale, flags)
 
 
-def plan_fft(x, region=None, *, BLUESTEIN_CUTOFF=DEFAULT_BLUESTEIN_CUTOFF, **_kwargs):
+FB_FLAG_GENERIC_ONLY = 1  # include/fftab200.h: generic kernels only (for tests)
+
+
+def plan_fft(x, region=None, *, BLUESTEIN_CUTOFF=DEFAULT_BLUESTEIN_CUTOFF, _flags=0, **_kwargs):
     """AbstractFFTs.plan_fft (FFTA src/plan.jl:71-72)."""
-    return _make_plan(x, region, FFT_FORWARD, BLUESTEIN_CUTOFF)
+    return _make_plan(x, region, FFT_FORWARD, BLUESTEIN_CUTOFF, flags=_flags)
 
 
-def plan_bfft(x, region=None, *, BLUESTEIN_CUTOFF=DEFAULT_BLUESTEIN_CUTOFF, **_kwargs):
+def plan_bfft(x, region=None, *, BLUESTEIN_CUTOFF=DEFAULT_BLUESTEIN_CUTOFF, _flags=0, **_kwargs):
     """AbstractFFTs.plan_bfft (FFTA src/plan.jl:74-75): unnormalised inverse."""
-    return _make_plan(x, region, FFT_BACKWARD, BLUESTEIN_CUTOFF)
+    return _make_plan(x, region, FFT_BACKWARD, BLUESTEIN_CUTOFF, flags=_flags)
 
 
-def plan_ifft(x, region=None, *, BLUESTEIN_CUTOFF=DEFAULT_BLUESTEIN_CUTOFF, **_kwargs):
+def plan_ifft(x, region=None, *, BLUESTEIN_CUTOFF=DEFAULT_BLUESTEIN_CUTOFF, _flags=0, **_kwargs):
     """AbstractFFTs.plan_ifft: plan_bfft scaled by 1/prod(sizes), fused in-kernel."""
-    return _make_plan(x, region, FFT_BACKWARD, BLUESTEIN_CUTOFF, scale_inverse=True)
+    return _make_plan(x, region, FFT_BACKWARD, BLUESTEIN_CUTOFF, scale_inverse=True,
+                      flags=_flags)
 
 
 def size(p: FFTAPlan_cx, i=None):

@@ -44,6 +44,11 @@ enum { FB_C32 = 0, FB_C64 = 1 };          /* ComplexF32, ComplexF64 */
 enum { FB_FORWARD = -1, FB_BACKWARD = 1 };
 enum { FB_DEFAULT_BLUESTEIN_CUTOFF = 73 }; /* src/callgraph.jl:44 */
 
+/* Plan flags.  FB_FLAG_GENERIC_ONLY: use only the generic line kernel, never
+ * the length-specialised ones (results are bit-identical either way; the
+ * flag exists so tests can check that). */
+enum { FB_FLAG_GENERIC_ONLY = 1u };
+
 /* Batched 1-D plan: `batch` transforms of length n; element j of transform b
  * is read at in[b*idist + j*istride] and written at out[b*odist + j*ostride].
  * Replaces plan_fft/plan_bfft with a one-dimensional region

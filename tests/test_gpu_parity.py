@@ -160,6 +160,28 @@ def test_twiddle_accuracy_bounds(N, bound):
     assert worst <= bound, worst
 
 
+FAST_LENGTHS = [2, 4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096, 8192, 16384, 3, 9, 27, 81,
+                243, 729, 2187, 6561, 1000]
+
+
+@pytest.mark.parametrize("n", FAST_LENGTHS)
+@pytest.mark.parametrize("dtype", [np.complex64, np.complex128])
+def test_specialised_equals_generic(n, dtype):
+    """The length-specialised kernels give the generic kernel's bits."""
+    import torch
+    rng = np.random.default_rng(n)
+    B = 5
+    x = torch.from_numpy(crandn(rng, (B, n), dtype)).cuda()
+    for planner in (F.plan_fft, F.plan_bfft, F.plan_ifft):
+        fast = planner(x.T, 1)
+        gen = planner(x.T, 1, _flags=F.FB_FLAG_GENERIC_ONLY)
+        a = (fast * x.T).T.cpu().numpy()
+        b = (gen * x.T).T.cpu().numpy()
+        assert np.array_equal(a, b), (n, planner.__name__, fast.describe(x.T), gen.describe(x.T))
+        ref = oracle.fft_nd(x.T.cpu().numpy(), 1, fast.dir, prec="f128") * fast.scale
+        assert relerr(a, ref.T) <= tol(dtype, n)
+
+
 # ----------------------------------------------------------------------- 2D
 @pytest.mark.parametrize("N", [8, 11, 15, 16, 27, 100])
 def test_delta_2d(N):
