@@ -39,7 +39,26 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 N = 4096
 BATCH = 16384
 ES = 8  # bytes per ComplexF32
-EXTRA = [(19683, 2 ** 24 // 19683), (27648, 2 ** 24 // 27648), (2 ** 20, 16)]
+# Other configurations, timed after the headline and reported under "extra":
+# (label, dtype, transform dims (Julia order), batch, region)
+EXTRA = [
+    ("c64_n1024_b1", "c64", (1024,), 1),
+    ("c32_n4096_b4096", "c32", (4096,), 4096),
+    ("c64_n4096_b4096", "c64", (4096,), 4096),
+    ("c32_n19683_b852", "c32", (19683,), 852),
+    ("c64_n19683_b852", "c64", (19683,), 852),
+    ("c32_n27648_b606", "c32", (27648,), 606),
+    ("c64_n27648_b606", "c64", (27648,), 606),
+    ("c32_n1048576_b16", "c32", (2 ** 20,), 16),
+    ("c64_n1048576_b16", "c64", (2 ** 20,), 16),
+    ("c32_n1009_b64", "c32", (1009,), 64),
+    ("c32_n65537_b16", "c32", (65537,), 16),
+    ("c32_n1000003_b1", "c32", (1000003,), 1),
+    ("c32_n1049344_b4", "c32", (2 ** 8 * 4099,), 4),
+    ("c32_2d_4096x4096", "c32", (4096, 4096), 1),
+    ("c32_2d_2187x2048", "c32", (2187, 2048), 1),
+    ("c32_2d_1000x1000", "c32", (1000, 1000), 1),
+]
 
 
 def flops(n, b):
@@ -164,6 +183,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--batch", type=int, default=BATCH,
                     help="columns per GPU (smaller for profiling captures)")
+    ap.add_argument("--workload", default=None,
+                    help="time one of the `extra` configurations instead of the headline "
+                         "(for profiling captures): " + ", ".join(e[0] for e in EXTRA))
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -195,12 +217,23 @@ def main():
 
     g = torch.Generator(device=dev)
     g.manual_seed(1234 + rank)
-    # Julia N x B column-major matrix = torch (B, N) row-major; columns contiguous
-    x = torch.complex(torch.randn(BATCH, N, device=dev, generator=g),
-                      torch.randn(BATCH, N, device=dev, generator=g))
+    label, kind, dims, batch = "headline", "c32", (N,), BATCH
+    if args.workload:
+        sel = [e for e in EXTRA if e[0] == args.workload]
+        if not sel:
+            raise SystemExit(f"unknown workload {args.workload}")
+        label, kind, dims, batch = sel[0]
+    es = 8 if kind == "c32" else 16
+    rdt = torch.float32 if kind == "c32" else torch.float64
+    # Julia's column-major (dims..., batch) array = torch row-major (batch, reversed dims)
+    shape = (batch,) + tuple(reversed(dims))
+    x = torch.complex(torch.randn(shape, device=dev, generator=g, dtype=rdt),
+                      torch.randn(shape, device=dev, generator=g, dtype=rdt))
     y = torch.empty_like(x)
-    p = F.plan_fft(x.T, 1)
-    xt, yt = x.T, y.T
+    perm = tuple(range(x.ndim - 1, -1, -1))
+    xt, yt = x.permute(perm), y.permute(perm)
+    p = F.plan_fft(xt, tuple(range(1, len(dims) + 1)))
+    n_tot = int(np.prod(dims))
     stream = torch.cuda.current_stream(dev)
 
     def step():
@@ -214,6 +247,13 @@ def main():
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
+        # keep the GPU busy with the same step for ~1 s so that the 100 ms clock
+        # samples cover the load, then time exactly K steps inside the same window
+        t_soak = time.perf_counter()
+        while time.perf_counter() - t_soak < 1.0:
+            for _ in range(20):
+                step()
+            torch.cuda.synchronize()
         ev0.record(stream)
         for _ in range(args.steps):
             step()
@@ -222,25 +262,28 @@ def main():
     barrier()
     ms = ev0.elapsed_time(ev1) / args.steps
     ms_max = max_over_ranks(ms)
-    total_flops = flops(N, BATCH) * world
+    total_flops = flops(n_tot, batch) * world
     value = total_flops / (ms_max * 1e-3) / 1e9
-    alg_bytes = 2.0 * N * BATCH * ES
+    alg_bytes = 2.0 * n_tot * batch * es
     achieved = alg_bytes / (ms * 1e-3) / 1e9
     peak, peak_kind = peaks()
 
     # accuracy spot check of this run against the FP64 oracle on a few columns
     import oracle
-    cols = [0, BATCH // 2, BATCH - 1]
+    cols = sorted({0, batch // 2, batch - 1})
     xs = x[cols].cpu().numpy().astype(np.complex128)
     ys = y[cols].cpu().numpy()
-    ref = oracle.fft_batched(xs, -1, nthreads=4)
+    if len(dims) == 1:
+        ref = oracle.fft_batched(xs, -1, nthreads=4)
+    else:
+        ref = np.stack([oracle.fft(np.asfortranarray(v.T), nthreads=4).T for v in xs])
     rel = float(np.linalg.norm(ys - ref) / np.linalg.norm(ref))
 
     # e2e: through the C ABI with host buffers (pinned), copies inside the timed region
     hx = x.cpu().pin_memory()
     hy = torch.empty_like(hx).pin_memory()
     hxn, hyn = hx.numpy(), hy.numpy()
-    ph = F.plan_fft(hxn.T, 1)
+    ph = F.plan_fft(hxn.T, tuple(range(1, len(dims) + 1)))
 
     def e2e_step():
         F.mul_(hyn.T, ph, hxn.T)
@@ -256,24 +299,37 @@ def main():
     e2e_value = total_flops / e2e_dt / 1e9
 
     extra = {}
-    if not args.no_extra and rank == 0:
-        for (n2, b2) in EXTRA:
-            xe = torch.complex(torch.randn(b2, n2, device=dev), torch.randn(b2, n2, device=dev))
+    if not args.no_extra and rank == 0 and not args.workload:
+        for (elabel, ekind, edims, b2) in EXTRA:
+            label_, kind_, dims_ = elabel, ekind, edims
+            ees = 8 if kind_ == "c32" else 16
+            erdt = torch.float32 if kind_ == "c32" else torch.float64
+            # row-major torch (b, dims reversed) = Julia column-major (dims..., b)
+            eshape = (b2,) + tuple(reversed(dims_))
+            xe = torch.complex(torch.randn(eshape, device=dev, dtype=erdt),
+                               torch.randn(eshape, device=dev, dtype=erdt))
             ye = torch.empty_like(xe)
-            pe = F.plan_fft(xe.T, 1)
+            perm = tuple(range(xe.ndim - 1, -1, -1))
+            xj, yj = xe.permute(perm), ye.permute(perm)
+            pe = F.plan_fft(xj, tuple(range(1, len(dims_) + 1)))
             for _ in range(3):
-                F.mul_(ye.T, pe, xe.T)
+                F.mul_(yj, pe, xj)
+            reps = 10
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            for _ in range(10):
-                F.mul_(ye.T, pe, xe.T)
+            for _ in range(reps):
+                F.mul_(yj, pe, xj)
             e1.record(stream)
             torch.cuda.synchronize()
-            t = e0.elapsed_time(e1) / 10
-            extra[f"c32_n{n2}_b{b2}"] = {
-                "ms": t, "GFLOP/s": flops(n2, b2) / (t * 1e-3) / 1e9,
-                "GB/s": 2.0 * n2 * b2 * ES / (t * 1e-3) / 1e9, "schedule": pe.describe(xe.T)}
-            del xe, ye, pe
+            t = e0.elapsed_time(e1) / reps
+            en = int(np.prod(dims_))
+            fl = 5.0 * en * np.log2(en) * b2
+            extra[label_] = {
+                "ms": t, "GFLOP/s": fl / (t * 1e-3) / 1e9,
+                "GB/s": 2.0 * en * b2 * ees / (t * 1e-3) / 1e9,
+                "frac_of_hbm": 2.0 * en * b2 * ees / (t * 1e-3) / 1e9 / peaks()[0],
+                "schedule": pe.describe(xj)}
+            del xe, ye, pe, xj, yj
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -285,13 +341,14 @@ def main():
                          f"split over {nthreads} threads, {dt:.1f} s"}
 
     if rank == 0:
+        wl = (f"batched C32 forward FFT, N={N}, {BATCH} contiguous columns per GPU"
+              if label == "headline" else f"{label} forward FFT")
         line = {
             "metric": "batched FFT GFLOP/s (5 N log2 N), C32 N=4096 x 16384",
             "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"batched C32 forward FFT, N={N}, {BATCH} contiguous columns "
-                                   "per GPU", "n": N, "batch_per_gpu": BATCH,
+            "config": {"workload": wl, "n": list(dims), "batch_per_gpu": batch,
                        "parallelism": f"batch-sharded x{world} (no collective)",
                        "l2": "inputs and outputs (512 MiB each) larger than L2; no flush",
                        "schedule": p.describe(xt)},
@@ -301,8 +358,8 @@ def main():
             "hbm_gbs": achieved,
             "rel_l2_vs_fp64_oracle": rel,
             "e2e": {"value": e2e_value, "unit": "GFLOP/s",
-                    "h2d_bytes_per_step": int(N * BATCH * ES),
-                    "d2h_bytes_per_step": int(N * BATCH * ES),
+                    "h2d_bytes_per_step": int(n_tot * batch * es),
+                    "d2h_bytes_per_step": int(n_tot * batch * es),
                     "path": "fb_execute_host from pinned host memory"},
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clk.summary(),

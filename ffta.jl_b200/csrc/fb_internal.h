@@ -77,11 +77,15 @@ struct FastFn {
   int L, T, nst;
   int radix[8];
   cudaError_t (*launch)(int dir, const FastArgs&, cudaStream_t);
-  cudaError_t (*launch_staged)(const LineArgs&, cudaStream_t);
+  cudaError_t (*launch_tile)(const LineArgs&, cudaStream_t);
   size_t lpad;
 };
-const FastFn* fast_table_f32(int* count);
-const FastFn* fast_table_f64(int* count);
+// The compiled specialised lengths of a type (dtype 0/1), in `parts` pieces.
+int fast_table_parts();
+const FastFn* fast_table(int dtype, int part, int* count);
+
+// Details of the last failed launch of a specialised kernel ("" if none).
+const char* last_launch_message();
 
 // Offsets (in (cos,sin) pairs) of each odd prime's table inside prime_cs.
 int prime_table_offset(int p);

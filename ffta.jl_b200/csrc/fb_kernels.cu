@@ -43,12 +43,38 @@ int prime_table_total() {
   return off;
 }
 
+const FastFn* fast_table_f32_0(int*);
+const FastFn* fast_table_f32_1(int*);
+const FastFn* fast_table_f32_2(int*);
+const FastFn* fast_table_f32_3(int*);
+const FastFn* fast_table_f64_0(int*);
+const FastFn* fast_table_f64_1(int*);
+const FastFn* fast_table_f64_2(int*);
+const FastFn* fast_table_f64_3(int*);
+
+int fast_table_parts() { return 4; }
+const FastFn* fast_table(int dtype, int part, int* count) {
+  typedef const FastFn* (*Get)(int*);
+  static const Get f32[4] = {fast_table_f32_0, fast_table_f32_1, fast_table_f32_2,
+                             fast_table_f32_3};
+  static const Get f64[4] = {fast_table_f64_0, fast_table_f64_1, fast_table_f64_2,
+                             fast_table_f64_3};
+  if (part < 0 || part >= 4) {
+    *count = 0;
+    return nullptr;
+  }
+  return (dtype == 0 ? f32 : f64)[part](count);
+}
+
 cudaError_t launch_line_f32_c16(const LineArgs&, size_t, cudaStream_t);
 cudaError_t launch_line_f32_c32(const LineArgs&, size_t, cudaStream_t);
 cudaError_t launch_line_f32_big(const LineArgs&, size_t, cudaStream_t);
 cudaError_t launch_line_f64_c16(const LineArgs&, size_t, cudaStream_t);
 cudaError_t launch_line_f64_c32(const LineArgs&, size_t, cudaStream_t);
 cudaError_t launch_line_f64_big(const LineArgs&, size_t, cudaStream_t);
+
+thread_local char g_launch_msg[512] = {0};
+const char* last_launch_message() { return g_launch_msg; }
 
 size_t line_smem_bytes(int dtype, const LineArgs& a) {
   const size_t es = dtype == 0 ? 8 : 16;

@@ -254,18 +254,20 @@ struct Pass {
   std::string what;
   const FastFn* fast = nullptr;    // specialised direct-I/O kernel, if any
   FastArgs fa;
-  const FastFn* staged = nullptr;  // specialised stage program with generic I/O
+  const FastFn* staged = nullptr;  // specialised tile kernel (strided lines, fused I/O)
 };
 
 // The specialised kernel for a radix program, if one is compiled.
 static const FastFn* find_fast(int dtype, int L, const std::vector<int>& radices) {
-  int cnt = 0;
-  const FastFn* t = dtype == FB_C32 ? fast_table_f32(&cnt) : fast_table_f64(&cnt);
-  for (int i = 0; i < cnt; ++i) {
-    if (t[i].L != L || t[i].nst != (int)radices.size()) continue;
-    bool same = true;
-    for (int s = 0; s < t[i].nst; ++s) same &= t[i].radix[s] == radices[s];
-    if (same) return &t[i];
+  for (int part = 0; part < fast_table_parts(); ++part) {
+    int cnt = 0;
+    const FastFn* t = fast_table(dtype, part, &cnt);
+    for (int i = 0; i < cnt; ++i) {
+      if (t[i].L != L || t[i].nst != (int)radices.size()) continue;
+      bool same = true;
+      for (int s = 0; s < t[i].nst; ++s) same &= t[i].radix[s] == radices[s];
+      if (same) return &t[i];
+    }
   }
   return nullptr;
 }
@@ -306,17 +308,28 @@ namespace fb {
 
 static int pick_G(const fb_plan_s* P, int L, int T, int Lpad, bool elem_major, int64_t nlines);
 
-// Switch a generic pass to the compile-time stage program of its length when
-// one is compiled (same arithmetic, no runtime radix dispatch).
-static void use_staged(const fb_plan_s* P, Pass& p, const std::vector<int>& radices) {
+// Switch a generic pass to the compile-time tile kernel of its length when
+// one is compiled (same arithmetic, direct HBM I/O, lines fastest across a
+// warp).  Bluestein passes need the forward-then-inverse order it implements.
+static void use_tile(const fb_plan_s* P, Pass& p, const std::vector<int>& radices) {
   if (P->flags & 1) return;
   const FastFn* ff = find_fast(P->dtype, p.a.prog.L, radices);
   if (!ff || (int)ff->lpad != p.a.Lpad) return;
-  p.staged = ff;
-  p.a.T = ff->T;
+  if (p.a.mid && (p.a.dir1 > 0 || p.a.dir2 < 0)) return;
+  const int es = elem_bytes(P->dtype);
+  const int T = ff->T;
+  const int thr_cap = std::max(1, std::max(512, T) / T);
+  const int smem_cap = (int)std::max<size_t>(1, (100 * 1024) / ((size_t)ff->lpad * es));
   const bool em = p.a.ld.mode == 1 || p.a.st.mode == 1;
-  p.a.G = pick_G(P, p.a.prog.L, ff->T, p.a.Lpad, em, p.a.nlines);
-  p.what += "[staged T=" + std::to_string(ff->T) + " G=" + std::to_string(p.a.G) + "]";
+  int want = std::max(1, 256 / T);
+  if (em) want = std::max(want, es == 8 ? 16 : 8);
+  int G = std::min(std::min(thr_cap, smem_cap), want);
+  const int64_t nl = std::max<int64_t>(1, p.a.nlines);
+  while (G > 1 && G / 2 >= nl) G /= 2;
+  p.staged = ff;
+  p.a.T = T;
+  p.a.G = std::max(1, G);
+  p.what += "[tile T=" + std::to_string(T) + " G=" + std::to_string(p.a.G) + "]";
 }
 
 static void* alloc_table(fb_plan_s* P, size_t bytes) {
@@ -389,7 +402,7 @@ static void blue_tables(fb_plan_s* P, int64_t N, int64_t M, void** pre, void** p
 
 static int pick_G(const fb_plan_s* P, int L, int T, int Lpad, bool elem_major, int64_t nlines) {
   const int es = elem_bytes(P->dtype);
-  const int thr_cap = std::max(1, line_max_threads() / T);
+  const int thr_cap = std::max(1, std::max(line_max_threads(), T) / T);
   const size_t line_bytes = (size_t)Lpad * es + 24;
   const size_t budget = 100 * 1024;
   int g_smem = (int)std::max<size_t>(1, budget / line_bytes);
@@ -566,8 +579,7 @@ static Axis plan_direct_axis(fb_plan_s* P, int64_t n, LineX& x, int64_t is, int6
     p.fa.prime_cs = p.a.prime_cs;
     p.fa.scale = 1.0;
     const int es = elem_bytes(P->dtype);
-    int G = std::max(1, 256 / ff->T);
-    G = std::min(G, std::max(1, line_max_threads() / ff->T));
+    int G = std::max(1, 256 / ff->T);  // 256-thread blocks (fb_fast.cuh DirectBounds)
     while (G > 1 && (size_t)G * ff->lpad * es > 100 * 1024) G /= 2;
     while (G > 1 && G / 2 >= nl) G /= 2;
     p.fa.G = G;
@@ -584,7 +596,7 @@ static Axis plan_direct_axis(fb_plan_s* P, int64_t n, LineX& x, int64_t is, int6
   for (size_t i = 0; i < x.radices.size(); ++i) w << (i ? "x" : "") << x.radices[i];
   w << " T=" << x.T << " G=" << p.a.G << " var=" << x.variant << ")";
   p.what = w.str();
-  use_staged(P, p, x.radices);
+  use_tile(P, p, x.radices);
   ax.passes.push_back(p);
   return ax;
 }
@@ -639,8 +651,8 @@ static Axis plan_four_axis(fb_plan_s* P, int64_t N, int64_t N1, int64_t N2, Line
      << " G=" << p2.a.G << ")";
   p1.what = w1.str();
   p2.what = w2.str();
-  use_staged(P, p1, x1.radices);
-  use_staged(P, p2, x2.radices);
+  use_tile(P, p1, x1.radices);
+  use_tile(P, p2, x2.radices);
   ax.passes.push_back(p1);
   ax.passes.push_back(p2);
   return ax;
@@ -733,9 +745,9 @@ static Axis plan_blue3_axis(fb_plan_s* P, int64_t N, int64_t is, int64_t os,
   p1.what = w.str() + ".1";
   p2.what = w.str() + ".2";
   p3.what = w.str() + ".3";
-  use_staged(P, p1, x1.radices);
-  use_staged(P, p2, x2.radices);
-  use_staged(P, p3, x1.radices);
+  use_tile(P, p1, x1.radices);
+  use_tile(P, p2, x2.radices);
+  use_tile(P, p3, x1.radices);
   ax.passes.push_back(p1);
   ax.passes.push_back(p2);
   ax.passes.push_back(p3);
@@ -896,12 +908,14 @@ static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s
           fa.in = a.in;
           fa.out = a.out;
           if (last) fa.scale = P->scale;
-          cuda_check(p.fast->launch(P->dir, fa, s), "fast kernel launch");
+          const cudaError_t e = p.fast->launch(P->dir, fa, s);
+          if (e != cudaSuccess) cuda_check(e, last_launch_message());
           continue;
         }
         if (last && P->scale != 1.0) a.scale = P->scale * a.scale;
         if (p.staged) {
-          cuda_check(p.staged->launch_staged(a, s), "staged kernel launch");
+          const cudaError_t e = p.staged->launch_tile(a, s);
+          if (e != cudaSuccess) cuda_check(e, last_launch_message());
           continue;
         }
         cuda_check(launch_line(P->dtype, p.variant, a, s), "line kernel launch");
