@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 #define FB_MAX_STAGES 24
 #define FB_MAX_PRIME 71  // largest prime done by a register butterfly
 
@@ -83,6 +85,9 @@ struct FastFn {
 // The compiled specialised lengths of a type (dtype 0/1), in `parts` pieces.
 int fast_table_parts();
 const FastFn* fast_table(int dtype, int part, int* count);
+
+// Set the message fb_last_error() returns on this thread.
+void set_last_error(const std::string& msg);
 
 // Details of the last failed launch of a specialised kernel ("" if none).
 const char* last_launch_message();

@@ -36,6 +36,7 @@
 namespace fb {
 
 static thread_local std::string g_last_error;
+void set_last_error(const std::string& msg) { g_last_error = msg; }
 
 struct FbError {
   int code;

@@ -43,6 +43,7 @@ SIGNATURES = {
     "fb_plan_describe": ([_vp, ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
     "fb_plan_destroy": ([_vp], ctypes.c_int),
     "fb_kernel_error_flag": ([ctypes.POINTER(ctypes.c_int), ctypes.c_int], ctypes.c_int),
+    "fb_execute_noalloc_c32": ([_vp, _vp, _i64, _i64, ctypes.c_int, _vp], ctypes.c_int),
     "fb_last_error": ([], ctypes.c_char_p),
     "fb_version": ([], ctypes.c_char_p),
 }

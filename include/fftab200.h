@@ -105,6 +105,23 @@ int fb_plan_describe(fb_plan plan, char* buf, size_t len);
 
 int fb_plan_destroy(fb_plan plan);
 
+/* Batched contiguous ComplexF32 transform that allocates no device memory:
+ * `batch` transforms of length n, element j of transform b at in[b*n + j] and
+ * out[b*n + j] (device pointers), direction dir, enqueued on `stream`.
+ * No counterpart in the reference (FFTA allocates its workspace while
+ * planning).  It exists for callers that cannot call cudaMalloc when they
+ * transform -- allocator callbacks, real-time loops that forbid allocation
+ * after start-up, hosts that hand over only the data buffers.  It runs the
+ * two-pass (four-step) schedule with its intermediate in a static device
+ * array of 4,194,304 complex values (32 MiB, held by every GPU that loads the
+ * library until exit) and its tables in a second static array.  Limits:
+ * n*batch <= 4194304 (else FB_ERR_ARGUMENT) and n a product of 2s, 3s and 5s
+ * (else FB_ERR_UNSUPPORTED).  All calls share the arrays: calls that overlap
+ * on the GPU race.  The first call on a device looks up the arrays' addresses
+ * (make it before any stream capture).  Errors via fb_last_error(). */
+int fb_execute_noalloc_c32(const void* in, void* out, int64_t n, int64_t batch, int dir,
+                           void* stream);
+
 /* Diagnostic: the current device's kernel error flag (0, or a radix that a
  * stage program named without a butterfly for it), optionally reset.  No
  * FFTA counterpart: FFTA raises ArgumentError("kernel not implemented")
