@@ -183,6 +183,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--batch", type=int, default=BATCH,
                     help="columns per GPU (smaller for profiling captures)")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving comparison")
     ap.add_argument("--workload", default=None,
                     help="time one of the `extra` configurations instead of the headline "
                          "(for profiling captures): " + ", ".join(e[0] for e in EXTRA))
@@ -331,6 +332,25 @@ def main():
                 "schedule": pe.describe(xj)}
             del xe, ye, pe, xj, yj
 
+    serving_out = None
+    if rank == 0 and world == 1 and not args.no_serving and not args.workload:
+        from ffta_b200 import serving as S
+        serving_out = {}
+        for name, kw in (("config5_bounded", dict(count=300, rates=(1e3, 1e4, 1e5, 0.0),
+                                                   n_max=2 ** 20, batch_max=512,
+                                                   max_elems=1 << 21)),
+                         ("small_requests", dict(count=3000, rates=(5e4, 2e5, 1e6, 0.0),
+                                                 n_max=4096, batch_max=16,
+                                                 max_elems=1 << 16))):
+            res = S.compare(**kw)
+            sat = res["sweep"][-1]
+            serving_out[name] = {
+                "saturated_throughput_ratio": sat["throughput_ratio"],
+                "saturated_p99_ms": {"batched": sat["batched"]["p99_ms"],
+                                     "one_launch_per_request":
+                                         sat["one_launch_per_request"]["p99_ms"]},
+                **res}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         nthreads = os.cpu_count() or 1
@@ -365,6 +385,7 @@ def main():
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
             "extra": extra,
+            "serving": serving_out,
         }
         print(json.dumps(line))
     if world > 1:

@@ -211,8 +211,24 @@ __global__ void __launch_bounds__(DirectBounds<R, T>::threads, DirectBounds<R, T
   const int64_t line = (int64_t)blockIdx.x * a.G + threadIdx.y;
   const bool ok = line < a.nlines;
   const int64_t l = ok ? line : 0;
-  const DirectIn<R> in{(const C*)a.in + l * a.idist, ok};
-  const DirectOut<R> out{(C*)a.out + l * a.odist, ok, (R)a.scale};
+  const C* gin = (const C*)a.in + l * a.idist;
+  C* gout = (C*)a.out + l * a.odist;
+  if (a.ndesc > 0) {
+    // grouped launch: find the request owning this line (binary search)
+    int lo = 0, hi = a.ndesc - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(a.pre + mid) <= l)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const int64_t k = l - __ldg(a.pre + lo);
+    gin = (const C*)a.ins[lo] + k * a.idist;
+    gout = (C*)a.outs[lo] + k * a.odist;
+  }
+  const DirectIn<R> in{gin, ok};
+  const DirectOut<R> out{gout, ok, (R)a.scale};
   fast_prog<R, DIR, RL, T>(buf, in, out, (const C*)a.tw, (const R*)a.prime_cs, threadIdx.x);
 }
 
@@ -237,7 +253,8 @@ __global__ void __launch_bounds__(T > 512 ? T : 512) fast_tile_kernel(const Line
   const TileIn<R> in{(const C*)a.in + (l0 * a.ld.s0 + l1 * a.ld.s1 + l2 * a.ld.s2), a.ld.es,
                      (const C*)a.ld.mul, a.ld.vn, a.ld.ves, l0 * a.ld.vls, ok};
   const TileOut<R> out{(C*)a.out + (l0 * a.st.s0 + l1 * a.st.s1 + l2 * a.st.s2), a.st.es,
-                       (const C*)a.st.mul, a.st.vn, a.st.ves, l0 * a.st.vls, l0,
+                       (const C*)a.st.mul, a.st.vn, a.st.ves, l0 * a.st.vls,
+                       a.tw_level ? l1 : l0,
                        a.tw_N ? (const C*)a.tw_hi : nullptr, (const C*)a.tw_lo, a.tw_shift,
                        a.tw_dir, (R)a.scale, ok};
   const C* tw = (const C*)a.prog.tw;

@@ -47,10 +47,11 @@ struct LineArgs {
   int dir2;             // direction of the second (only with mid)
   const void* mid;      // pointwise multiplier between the two transforms, or null
   int64_t mid_ls, mid_es;
-  // twiddle on store: multiply element k of line l by w_N^(dir * l0 * k),
+  // twiddle on store: multiply element k of line l by w_N^(dir * lt * k) where
+  // lt is the line's level-`tw_level` index (l0 or l1),
   // w_N^e = hi[e >> shift] * lo[e & (2^shift - 1)].
   int64_t tw_N;         // 0: none
-  int tw_dir, tw_shift;
+  int tw_dir, tw_shift, tw_level;
   const void* tw_hi;
   const void* tw_lo;
   double scale;         // applied on store when != 1
@@ -71,6 +72,14 @@ struct FastArgs {
   const void* prime_cs;
   double scale;
   int G;
+  // Grouped launch (ndesc > 0): the lines of ndesc requests in one launch.
+  // Request r owns lines pre[r] .. pre[r+1]-1, its line l at
+  // ins[r] + (l - pre[r])*idist and outs[r] + (l - pre[r])*odist; `in` and
+  // `out` are unused.  The descriptor arrays live in device memory.
+  int ndesc;
+  const int64_t* pre;
+  const void* const* ins;
+  void* const* outs;
 };
 
 // One specialised length: its radix program, threads per line, launcher and
@@ -99,6 +108,9 @@ int prime_table_total();
 // Kernel launch entry points (fb_kernels.cu).  dtype: 0 = C32, 1 = C64.
 cudaError_t launch_line(int dtype, int variant, const LineArgs& a, cudaStream_t s);
 size_t line_smem_bytes(int dtype, const LineArgs& a);
+// Work-descriptor launch of the generic kernel (see line_kernel_desc).
+cudaError_t launch_desc(int dtype, int variant, const LineArgs* descs, const int64_t* bstart,
+                        int ndesc, int64_t nblocks, int threads, size_t smem, cudaStream_t s);
 int line_max_threads();
 // variant bits: 1 = large register budget (32 values/thread), 2 = big primes
 cudaError_t gen_stage_twiddles(int dtype, void* out, int R, int64_t Ns, cudaStream_t s);

@@ -66,6 +66,30 @@ const FastFn* fast_table(int dtype, int part, int* count) {
   return (dtype == 0 ? f32 : f64)[part](count);
 }
 
+#define FB_DESC_DECL(tag)                                                                 \
+  cudaError_t launch_desc_##tag(const LineArgs*, const int64_t*, int, int64_t, int, size_t, \
+                                cudaStream_t);
+FB_DESC_DECL(f32_c16)
+FB_DESC_DECL(f32_c32)
+FB_DESC_DECL(f32_big)
+FB_DESC_DECL(f64_c16)
+FB_DESC_DECL(f64_c32)
+FB_DESC_DECL(f64_big)
+#undef FB_DESC_DECL
+
+cudaError_t launch_desc(int dtype, int variant, const LineArgs* descs, const int64_t* bstart,
+                        int ndesc, int64_t nblocks, int threads, size_t smem, cudaStream_t s) {
+  const bool cap32 = variant & 1, big = variant & 2;
+  if (dtype == 0) {
+    if (big) return launch_desc_f32_big(descs, bstart, ndesc, nblocks, threads, smem, s);
+    return cap32 ? launch_desc_f32_c32(descs, bstart, ndesc, nblocks, threads, smem, s)
+                 : launch_desc_f32_c16(descs, bstart, ndesc, nblocks, threads, smem, s);
+  }
+  if (big) return launch_desc_f64_big(descs, bstart, ndesc, nblocks, threads, smem, s);
+  return cap32 ? launch_desc_f64_c32(descs, bstart, ndesc, nblocks, threads, smem, s)
+               : launch_desc_f64_c16(descs, bstart, ndesc, nblocks, threads, smem, s);
+}
+
 cudaError_t launch_line_f32_c16(const LineArgs&, size_t, cudaStream_t);
 cudaError_t launch_line_f32_c32(const LineArgs&, size_t, cudaStream_t);
 cudaError_t launch_line_f32_big(const LineArgs&, size_t, cudaStream_t);
@@ -78,7 +102,7 @@ const char* last_launch_message() { return g_launch_msg; }
 
 size_t line_smem_bytes(int dtype, const LineArgs& a) {
   const size_t es = dtype == 0 ? 8 : 16;
-  return (size_t)a.G * a.Lpad * es + (size_t)3 * a.G * sizeof(int64_t);
+  return (size_t)a.G * a.Lpad * es + (size_t)4 * a.G * sizeof(int64_t);
 }
 int line_max_threads() { return 512; }
 

@@ -162,7 +162,7 @@ __device__ __forceinline__ void run_prog(cplx<R>* buf, const StageProg& p, const
 // ------------------------------------------------------------ load / store
 template <typename R>
 __device__ __forceinline__ void load_lines(const LineArgs& a, cplx<R>* sm, const int64_t* lb,
-                                           int64_t line0, int tid, int nthr) {
+                                           int64_t line0, int tid, int nthr, int u, int gl) {
   typedef cplx<R> C;
   const C* __restrict__ in = (const C*)a.in;
   const LineIO& io = a.ld;
@@ -184,10 +184,10 @@ __device__ __forceinline__ void load_lines(const LineArgs& a, cplx<R>* sm, const
       sm[g * Lp + padi(i)] = v;
     }
   } else {
-    const int g = threadIdx.y, T = a.T;
+    const int g = gl, T = a.T;
     const bool ok = line0 + g < a.nlines;
     const int64_t base = lb[g], l0 = lb[2 * G + g];
-    for (int i = threadIdx.x; i < L; i += T) {
+    for (int i = u; i < L; i += T) {
       C v = zero;
       if (ok && i < cnt) {
         const int64_t vi = (int64_t)i * io.ves + l0 * io.vls;
@@ -202,12 +202,12 @@ __device__ __forceinline__ void load_lines(const LineArgs& a, cplx<R>* sm, const
 }
 
 template <typename R>
-__device__ __forceinline__ cplx<R> finish(const LineArgs& a, cplx<R> v, int64_t l0, int i,
+__device__ __forceinline__ cplx<R> finish(const LineArgs& a, cplx<R> v, int64_t tfac, int i,
                                           int64_t vi) {
   typedef cplx<R> C;
   if (a.st.mul) v = cmul<R>(v, __ldg((const C*)a.st.mul + vi));
   if (a.tw_N) {
-    const int64_t e = l0 * (int64_t)i;
+    const int64_t e = tfac * (int64_t)i;
     const C hi = __ldg((const C*)a.tw_hi + (e >> a.tw_shift));
     const C lo = __ldg((const C*)a.tw_lo + (e & ((int64_t(1) << a.tw_shift) - 1)));
     const C w = cmul<R>(hi, lo);
@@ -219,7 +219,8 @@ __device__ __forceinline__ cplx<R> finish(const LineArgs& a, cplx<R> v, int64_t 
 
 template <typename R>
 __device__ __forceinline__ void store_lines(const LineArgs& a, const cplx<R>* sm,
-                                            const int64_t* lb, int64_t line0, int tid, int nthr) {
+                                            const int64_t* lb, int64_t line0, int tid, int nthr,
+                                            int u, int gl) {
   typedef cplx<R> C;
   C* __restrict__ out = (C*)a.out;
   const LineIO& io = a.st;
@@ -232,30 +233,35 @@ __device__ __forceinline__ void store_lines(const LineArgs& a, const cplx<R>* sm
       const int64_t l0 = lb[2 * G + g];
       const int64_t vi = (int64_t)i * io.ves + l0 * io.vls;
       if (vi >= io.vn) continue;
-      out[lb[G + g] + (int64_t)i * io.es] = finish<R>(a, sm[g * Lp + padi(i)], l0, i, vi);
+      out[lb[G + g] + (int64_t)i * io.es] = finish<R>(a, sm[g * Lp + padi(i)], lb[3 * G + g], i, vi);
     }
   } else {
-    const int g = threadIdx.y, T = a.T;
+    const int g = gl, T = a.T;
     if (line0 + g >= a.nlines) return;
-    const int64_t base = lb[G + g], l0 = lb[2 * G + g];
-    for (int i = threadIdx.x; i < cnt; i += T) {
+    const int64_t base = lb[G + g], l0 = lb[2 * G + g], tfac = lb[3 * G + g];
+    for (int i = u; i < cnt; i += T) {
       const int64_t vi = (int64_t)i * io.ves + l0 * io.vls;
       if (vi >= io.vn) continue;
-      out[base + (int64_t)i * io.es] = finish<R>(a, sm[g * Lp + padi(i)], l0, i, vi);
+      out[base + (int64_t)i * io.es] = finish<R>(a, sm[g * Lp + padi(i)], tfac, i, vi);
     }
   }
 }
 
 // ----------------------------------------------------------------- kernel
+// One block's work: lines block*G .. block*G + G-1 of `a`.  Thread (u, g) is
+// butterfly lane u of line g; tid = g*T + u.  Threads of a block beyond T*G
+// pass u = kIdle (no butterflies, no elements) and tid = T*G, and only take
+// part in the barriers.
+constexpr int kIdle = 1 << 29;
+
 template <typename R, int CAP, bool BIG>
-__global__ void __launch_bounds__(512) line_kernel(const LineArgs a) {
+__device__ __forceinline__ void line_body(const LineArgs& a, int64_t block, int u, int g, int tid,
+                                          unsigned char* smraw) {
   typedef cplx<R> C;
-  extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = (C*)smraw;
   const int T = a.T, G = a.G;
-  const int u = threadIdx.x, g = threadIdx.y;
-  const int tid = g * T + u, nthr = G * T;
-  const int64_t line0 = (int64_t)blockIdx.x * G;
+  const int nthr = G * T;
+  const int64_t line0 = block * G;
   int64_t* lb = (int64_t*)(sm + (size_t)G * a.Lpad);
   if (tid < G) {
     const int64_t l = line0 + tid;
@@ -264,9 +270,10 @@ __global__ void __launch_bounds__(512) line_kernel(const LineArgs a) {
     lb[tid] = l0 * a.ld.s0 + l1 * a.ld.s1 + l2 * a.ld.s2;
     lb[G + tid] = l0 * a.st.s0 + l1 * a.st.s1 + l2 * a.st.s2;
     lb[2 * G + tid] = l0;
+    lb[3 * G + tid] = a.tw_level ? l1 : l0;
   }
   __syncthreads();
-  load_lines<R>(a, sm, lb, line0, tid, nthr);
+  load_lines<R>(a, sm, lb, line0, tid, nthr, u, g);
   __syncthreads();
   C* buf = sm + g * a.Lpad;
   const R* pcs = (const R*)a.prime_cs;
@@ -287,7 +294,45 @@ __global__ void __launch_bounds__(512) line_kernel(const LineArgs a) {
       __syncthreads();
     }
   }
-  store_lines<R>(a, sm, lb, line0, tid, nthr);
+  store_lines<R>(a, sm, lb, line0, tid, nthr, u, g);
+}
+
+template <typename R, int CAP, bool BIG>
+__global__ void __launch_bounds__(512) line_kernel(const LineArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int u = threadIdx.x, g = threadIdx.y;
+  line_body<R, CAP, BIG>(a, blockIdx.x, u, g, g * a.T + u, smraw);
+}
+
+// Work-descriptor launch: many line transforms -- different lengths,
+// directions, pointers -- in one grid.  Descriptor r owns blocks
+// bstart[r] .. bstart[r+1]-1 and is run by the generic body with its own
+// T x G shape inside the launch's one-dimensional block.
+template <typename R, int CAP, bool BIG>
+__global__ void __launch_bounds__(512)
+    line_kernel_desc(const LineArgs* __restrict__ descs, const int64_t* __restrict__ bstart,
+                     int ndesc) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ LineArgs sa;
+  __shared__ int64_t sblock;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = ndesc - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(bstart + mid) <= (int64_t)blockIdx.x)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    sa = descs[lo];
+    sblock = (int64_t)blockIdx.x - __ldg(bstart + lo);
+  }
+  __syncthreads();
+  const int nthr = sa.T * sa.G;
+  const bool active = (int)threadIdx.x < nthr;
+  const int u = active ? (int)threadIdx.x % sa.T : kIdle;
+  const int g = active ? (int)threadIdx.x / sa.T : 0;
+  line_body<R, CAP, BIG>(sa, sblock, u, g, active ? (int)threadIdx.x : nthr, smraw);
 }
 
 }  // namespace fb

@@ -27,4 +27,24 @@ cudaError_t FB_LAUNCH(const LineArgs& a, size_t smem, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// Launch ndesc descriptors (device arrays) as one grid of `nblocks` blocks of
+// `threads` threads with `smem` bytes of dynamic shared memory each.
+cudaError_t FB_LAUNCH_DESC(const LineArgs* descs, const int64_t* bstart, int ndesc,
+                           int64_t nblocks, int threads, size_t smem, cudaStream_t s) {
+  static int set_bytes[64] = {0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (smem > 48 * 1024 && (dev >= 64 || set_bytes[dev] < (int)smem)) {
+    e = cudaFuncSetAttribute(line_kernel_desc<FB_R, FB_CAP, FB_BIG>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    if (e != cudaSuccess) return e;
+    if (dev < 64) set_bytes[dev] = 220 * 1024;
+  }
+  if (nblocks <= 0 || ndesc <= 0) return cudaSuccess;
+  line_kernel_desc<FB_R, FB_CAP, FB_BIG><<<dim3((unsigned)nblocks), dim3(threads), smem, s>>>(
+      descs, bstart, ndesc);
+  return cudaGetLastError();
+}
+
 }  // namespace fb

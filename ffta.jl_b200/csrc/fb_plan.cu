@@ -21,7 +21,9 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <deque>
 #include <map>
+#include <tuple>
 #include <memory>
 #include <mutex>
 #include <sstream>
@@ -289,7 +291,7 @@ struct Axis {
 
 struct fb_plan_s {
   int dtype = 0, dir = -1, device = 0;
-  uint32_t flags = 0;  // bit 0: generic kernels only (no specialised lengths)
+  uint32_t flags = 0;  // FB_FLAG_GENERIC_ONLY, FB_FLAG_SAME_SCHEDULE_STRIDED
   int64_t cutoff = 73;
   double scale = 1.0;
   int rank = 0;
@@ -301,6 +303,8 @@ struct fb_plan_s {
   std::unique_ptr<fb::DevBuf> scratch0, scratch1;
   // host-execution staging
   std::unique_ptr<fb::DevBuf> hin, hout;
+  // grouped execution: device copy of the request descriptors
+  std::unique_ptr<fb::DevBuf> desc;
   int64_t in_span = 0, out_span = 0;
   size_t table_bytes = 0;
 };
@@ -605,6 +609,20 @@ static Axis plan_direct_axis(fb_plan_s* P, int64_t n, LineX& x, int64_t is, int6
 // Four-step N = N1*N2: pass 1 transforms the N2 strided columns (length N1)
 // into scratch with the twiddle w_N^(n2 k1) fused; pass 2 transforms the N1
 // rows (length N2) and writes X[k1 + N1 k2].
+//
+// Line order.  For an axis whose elements are contiguous (is == 1) the lines
+// of a pass are ordered (n2 or k1, batch...): neighbouring lines are
+// neighbouring in memory.  For a strided axis whose first batch dim is
+// contiguous (the columns of a 2-D array) they are ordered (batch0, n2 or
+// k1, batch1) instead, the scratch keeps batch0 fastest, and the twiddle's
+// line factor is the level-1 index -- again neighbouring lines are
+// neighbouring in memory, so both passes move long contiguous runs.
+//
+// L2 residency.  With contiguous axes the batch is cut into chunks whose
+// scratch (N * chunk elements, at most kL2Chunk bytes) stays in L2 between
+// pass 1 and pass 2; the chunks run one after the other (host loop).
+static const size_t kL2Chunk = 32u << 20;
+
 static Axis plan_four_axis(fb_plan_s* P, int64_t N, int64_t N1, int64_t N2, LineX& x1, LineX& x2,
                            int64_t is, int64_t os, const std::vector<BDim>& bd, int src, int dst) {
   Axis ax;
@@ -612,44 +630,85 @@ static Axis plan_four_axis(fb_plan_s* P, int64_t N, int64_t N1, int64_t N2, Line
   ax.kind = "FOUR";
   std::vector<BDim> inner;
   split_levels(bd, 2, &inner, &ax.outer);
-  const int64_t B = prod_n(inner, 0, 2), B0 = level_n(inner, 0);
+  const bool tmode = is != 1 && !inner.empty() && inner[0].is == 1 && inner[0].os == 1 &&
+                     inner[0].n > 1;
+  const int es = elem_bytes(P->dtype);
+  if (!tmode && !inner.empty()) {
+    // chunk the first batch dim so that N * chunk elements fit kL2Chunk
+    const int64_t B0 = inner[0].n;
+    const int64_t per = std::max<int64_t>(1, (int64_t)(kL2Chunk / ((size_t)N * es)));
+    if (B0 > per) {
+      int64_t chunk = 1;
+      for (int64_t c = per; c >= 1; --c)
+        if (B0 % c == 0) {
+          chunk = c;
+          break;
+        }
+      if (chunk * 4 >= per) {  // only when the chunk is not tiny
+        ax.outer.insert(ax.outer.begin(),
+                        BDim{B0 / chunk, chunk * inner[0].is, chunk * inner[0].os});
+        inner[0].n = chunk;
+        ax.kind = "FOUR/L2";
+      }
+    }
+  }
+  const int64_t B = prod_n(inner, 0, 2), B0 = level_n(inner, 0), B1 = level_n(inner, 1);
   P->scratch_elems = std::max<size_t>(P->scratch_elems, (size_t)(N * B));
-  // pass 1
-  Pass p1;
+  Pass p1, p2;
   base_args(P, x1, &p1.a, P->dir);
+  base_args(P, x2, &p2.a, P->dir);
   p1.variant = x1.variant;
+  p2.variant = x2.variant;
   p1.src = src;
   p1.dst = B_S0;
-  p1.a.nlines = N2 * B;
-  p1.a.m0 = N2;
-  p1.a.m1 = B0;
-  p1.a.ld = io_plain(is, level_is(inner, 0), level_is(inner, 1), N2 * is, x1.L);
-  p1.a.st = io_plain(1, N, B0 * N, N2, x1.L);
-  if (x1.kind == 1) attach_blue(P, x1, &p1.a);
-  attach_twiddle(P, &p1.a, N, P->dir);
-  p1.a.ld.mode = is == 1 ? 1 : 0;
-  p1.a.st.mode = 1;
-  p1.a.G = pick_G(P, x1.L, x1.T, p1.a.Lpad, true, p1.a.nlines);
-  // pass 2
-  Pass p2;
-  base_args(P, x2, &p2.a, P->dir);
-  p2.variant = x2.variant;
   p2.src = B_S0;
   p2.dst = dst;
+  p1.a.nlines = N2 * B;
   p2.a.nlines = N1 * B;
-  p2.a.m0 = N1;
-  p2.a.m1 = B0;
-  p2.a.ld = io_plain(N2, N, B0 * N, 1, x2.L);
-  p2.a.st = io_plain(os, level_os(inner, 0), level_os(inner, 1), N1 * os, x2.L);
+  if (!tmode) {
+    // lines (n2, b0, b1); scratch S[b*N + k1*N2 + n2], b = b0 + B0*b1
+    p1.a.m0 = N2;
+    p1.a.m1 = B0;
+    p1.a.ld = io_plain(is, level_is(inner, 0), level_is(inner, 1), N2 * is, x1.L);
+    p1.a.st = io_plain(1, N, B0 * N, N2, x1.L);
+    p1.a.ld.mode = is == 1 ? 1 : 0;
+    p1.a.st.mode = 1;
+    // lines (k1, b0, b1)
+    p2.a.m0 = N1;
+    p2.a.m1 = B0;
+    p2.a.ld = io_plain(N2, N, B0 * N, 1, x2.L);
+    p2.a.st = io_plain(os, level_os(inner, 0), level_os(inner, 1), N1 * os, x2.L);
+    p2.a.ld.mode = 0;
+    p2.a.st.mode = os == 1 ? 1 : 0;
+  } else {
+    // lines (b0, n2, b1); scratch S[b0 + B0*(k1*N2 + n2) + B0*N*b1]
+    p1.a.m0 = B0;
+    p1.a.m1 = N2;
+    p1.a.ld = io_plain(1, is, level_is(inner, 1), N2 * is, x1.L);
+    p1.a.st = io_plain(1, B0, B0 * N, B0 * N2, x1.L);
+    p1.a.ld.mode = 1;
+    p1.a.st.mode = 1;
+    // lines (b0, k1, b1)
+    p2.a.m0 = B0;
+    p2.a.m1 = N1;
+    p2.a.ld = io_plain(1, B0 * N2, B0 * N, B0, x2.L);
+    p2.a.st = io_plain(1, os, level_os(inner, 1), N1 * os, x2.L);
+    p2.a.ld.mode = 1;
+    p2.a.st.mode = 1;
+    (void)B1;
+  }
+  if (x1.kind == 1) attach_blue(P, x1, &p1.a);
   if (x2.kind == 1) attach_blue(P, x2, &p2.a);
-  p2.a.ld.mode = 0;
-  p2.a.st.mode = os == 1 ? 1 : 0;
-  p2.a.G = pick_G(P, x2.L, x2.T, p2.a.Lpad, p2.a.st.mode == 1, p2.a.nlines);
+  attach_twiddle(P, &p1.a, N, P->dir);
+  p1.a.tw_level = tmode ? 1 : 0;
+  p1.a.G = pick_G(P, x1.L, x1.T, p1.a.Lpad, true, p1.a.nlines);
+  p2.a.G = pick_G(P, x2.L, x2.T, p2.a.Lpad, p2.a.ld.mode == 1 || p2.a.st.mode == 1,
+                  p2.a.nlines);
   std::ostringstream w1, w2;
-  w1 << "FOUR.1(N1=" << N1 << (x1.kind ? " blue" : "") << " L=" << x1.L << " T=" << x1.T
-     << " G=" << p1.a.G << ")";
-  w2 << "FOUR.2(N2=" << N2 << (x2.kind ? " blue" : "") << " L=" << x2.L << " T=" << x2.T
-     << " G=" << p2.a.G << ")";
+  w1 << "FOUR" << (tmode ? "T" : "") << ".1(N1=" << N1 << (x1.kind ? " blue" : "")
+     << " L=" << x1.L << " T=" << x1.T << " G=" << p1.a.G << ")";
+  w2 << "FOUR" << (tmode ? "T" : "") << ".2(N2=" << N2 << (x2.kind ? " blue" : "")
+     << " L=" << x2.L << " T=" << x2.T << " G=" << p2.a.G << ")";
   p1.what = w1.str();
   p2.what = w2.str();
   use_tile(P, p1, x1.radices);
@@ -760,7 +819,19 @@ static Axis plan_axis(fb_plan_s* P, int64_t n, int64_t is, int64_t os, std::vect
   if (n <= 0) fail(FB_ERR_DIMENSION_MISMATCH, "Array length must be strictly positive");
   bd = normalize_batch(bd);
   LineX x;
-  if (make_direct(n, P->cutoff, P->dtype, &x)) return plan_direct_axis(P, n, x, is, os, bd, src, dst);
+  // A strided axis whose neighbouring lines are neighbours in memory: one
+  // pass holds only as many lines as fit shared memory, so a long line gives
+  // short contiguous runs.  Below 128-byte runs prefer a four-step split whose
+  // passes hold many lines (FOURT order, see plan_four_axis).
+  const bool strided = is != 1 && !bd.empty() && bd[0].is == 1 && bd[0].os == 1 && bd[0].n > 1;
+  bool prefer_split = false;
+  if (strided && make_direct(n, P->cutoff, P->dtype, &x)) {
+    const int es = elem_bytes(P->dtype);
+    const int lines = std::max(1, (int)((100 * 1024) / ((size_t)lpad_for(x.L) * es)));
+    prefer_split = (int64_t)std::min(lines, 16) * es < 128 && !(P->flags & FB_FLAG_SAME_SCHEDULE_STRIDED);
+  }
+  if (!prefer_split && make_direct(n, P->cutoff, P->dtype, &x))
+    return plan_direct_axis(P, n, x, is, os, bd, src, dst);
   // Bluestein for a prime in one kernel when its pad fits.
   if (is_prime(n) && make_blue1(n, P->dtype, &x))
     return plan_direct_axis(P, n, x, is, os, bd, src, dst);
@@ -775,6 +846,7 @@ static Axis plan_axis(fb_plan_s* P, int64_t n, int64_t is, int64_t os, std::vect
       const int64_t a = cand[o], b = n / a;
       LineX xa, xb;
       if (!make_line(a, P->cutoff, P->dtype, &xa) || !make_line(b, P->cutoff, P->dtype, &xb)) continue;
+      if (prefer_split && (xa.kind != 0 || xb.kind != 0)) continue;
       double c = line_cost(xa) * (double)b + line_cost(xb) * (double)a;
       // prefer balanced direct splits on ties
       c *= 1.0 + 1e-9 * std::fabs(std::log((double)a) - std::log((double)b));
@@ -787,6 +859,8 @@ static Axis plan_axis(fb_plan_s* P, int64_t n, int64_t is, int64_t os, std::vect
     }
   }
   if (bN1) return plan_four_axis(P, n, bN1, n / bN1, b1, b2, is, os, bd, src, dst);
+  if (prefer_split && make_direct(n, P->cutoff, P->dtype, &x))
+    return plan_direct_axis(P, n, x, is, os, bd, src, dst);
   return plan_blue3_axis(P, n, is, os, bd, src, dst);
 }
 
@@ -1022,6 +1096,57 @@ int fb_execute_host(fb_plan plan, const void* in, void* out, void* stream) {
   });
 }
 
+int fb_execute_grouped(fb_plan plan, int64_t count, const void* const* ins, void* const* outs,
+                       const int64_t* batches, void* stream) {
+  return guard([&] {
+    if (!plan || (count > 0 && (!ins || !outs || !batches))) fail(FB_ERR_ARGUMENT, "null argument");
+    if (count <= 0) return;
+    if (plan->axes.size() != 1 || plan->axes[0].passes.size() != 1 ||
+        !plan->axes[0].passes[0].fast || !plan->axes[0].outer.empty())
+      fail(FB_ERR_UNSUPPORTED, "grouped execution needs a plan of one single-pass batched length");
+    const Pass& p = plan->axes[0].passes[0];
+    const int64_t n = plan->axes[0].n;
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev != plan->device) fail(FB_ERR_ARGUMENT, "plan was created on another device");
+    // descriptor block: pre[count+1] | ins[count] | outs[count]
+    std::vector<int64_t> blob((size_t)(3 * count + 1));
+    int64_t total = 0;
+    for (int64_t r = 0; r < count; ++r) {
+      if (batches[r] < 0) fail(FB_ERR_DIMENSION_MISMATCH, "negative batch");
+      blob[r] = total;
+      total += batches[r];
+      blob[count + 1 + r] = (int64_t)(uintptr_t)ins[r];
+      blob[2 * count + 1 + r] = (int64_t)(uintptr_t)outs[r];
+    }
+    blob[count] = total;
+    if (total == 0) return;
+    const size_t bytes = blob.size() * sizeof(int64_t);
+    if (!plan->desc || plan->desc->bytes < bytes) plan->desc.reset(new DevBuf(bytes * 2));
+    cudaStream_t s = (cudaStream_t)stream;
+    cuda_check(cudaMemcpyAsync(plan->desc->p, blob.data(), bytes, cudaMemcpyHostToDevice, s),
+               "descriptor copy");
+    const int64_t* d = (const int64_t*)plan->desc->p;
+    FastArgs fa = p.fa;
+    fa.in = nullptr;
+    fa.out = nullptr;
+    fa.idist = n;  // each request's transforms are contiguous (API contract)
+    fa.odist = n;
+    fa.nlines = total;
+    fa.scale = plan->scale;
+    fa.ndesc = (int)count;
+    fa.pre = d;
+    fa.ins = (const void* const*)(d + count + 1);
+    fa.outs = (void* const*)(d + 2 * count + 1);
+    const int es = elem_bytes(plan->dtype);
+    int G = std::max(1, 256 / p.fast->T);
+    while (G > 1 && (size_t)G * p.fast->lpad * es > 100 * 1024) G /= 2;
+    fa.G = G;
+    const cudaError_t e = p.fast->launch(plan->dir, fa, s);
+    if (e != cudaSuccess) cuda_check(e, last_launch_message());
+  });
+}
+
 int fb_plan_size(fb_plan plan, int i, int64_t* out) {
   return guard([&] {
     if (!plan || !out) fail(FB_ERR_ARGUMENT, "null argument");
@@ -1075,5 +1200,367 @@ int fb_kernel_error_flag(int* value, int reset) {
 
 const char* fb_last_error(void) { return g_last_error.c_str(); }
 const char* fb_version(void) { return FB_VERSION; }
+
+}  // extern "C"
+
+// ===================================================================== server
+// Continuous batching over work-descriptor launches.  Requests (n, type,
+// direction, batch, device in/out) wait in arrival order; dispatch() admits
+// them while their bytes fit the budget and
+//  * packs every admitted request whose length runs in one pass into
+//    work-descriptor launches of the generic kernel (one per kernel variant,
+//    block size and shared-memory class) -- requests of different lengths and
+//    directions share a launch;
+//  * runs multi-pass lengths (four-step, three-pass Bluestein) with a cached
+//    per-(n, type, direction, batch) plan on one dedicated stream, so that
+//    their plan-owned scratch is never used by two requests at once.
+// Launches rotate over the server's streams; poll() retires completed ones
+// and dispatches what has arrived since, so new requests join as earlier
+// ones finish.
+namespace fb {
+
+struct SrvReq {
+  int64_t ticket, n, batch;
+  int dtype, dir;
+  const void* in;
+  void* out;
+  double bytes;
+};
+
+struct SrvLaunch {
+  cudaEvent_t ev;
+  std::vector<int64_t> tickets;
+  double bytes;
+  int slot;  // descriptor slot, or -1
+};
+
+struct SrvSlot {
+  std::unique_ptr<DevBuf> buf;
+  void* host = nullptr;  // pinned staging of the descriptor table
+  size_t host_bytes = 0;
+  cudaEvent_t last = nullptr;  // the launch that last read this slot
+};
+
+}  // namespace fb
+
+struct fb_server_s {
+  int device = 0;
+  double budget = 100e9;
+  std::vector<cudaStream_t> streams;
+  cudaStream_t serial = nullptr;  // multi-pass plans
+  cudaEvent_t start = nullptr;
+  int next_stream = 0, next_slot = 0;
+  std::map<std::tuple<int64_t, int, int>, std::unique_ptr<fb_plan_s>> templ;
+  std::map<std::tuple<int64_t, int, int, int64_t>, std::unique_ptr<fb_plan_s>> multi;
+  std::deque<fb::SrvReq> pending;
+  std::deque<fb::SrvLaunch> inflight;
+  std::vector<fb::SrvSlot> slots;
+  double admitted = 0;
+  int64_t next_ticket = 0;
+  std::vector<std::pair<int64_t, double>> done;
+  int64_t st_launches = 0, st_desc_launches = 0, st_requests = 0, st_max_queue = 0;
+  double st_max_admitted = 0;
+  ~fb_server_s() {
+    for (auto& l : inflight) cudaEventDestroy(l.ev);
+    for (auto& sl : slots) {
+      if (sl.last) cudaEventDestroy(sl.last);
+      if (sl.host) cudaFreeHost(sl.host);
+    }
+    for (auto s : streams) cudaStreamDestroy(s);
+    if (serial) cudaStreamDestroy(serial);
+    if (start) cudaEventDestroy(start);
+  }
+};
+
+namespace fb {
+
+static fb_plan_s* srv_template(fb_server_s* S, int64_t n, int dtype, int dir) {
+  auto key = std::make_tuple(n, dtype, dir);
+  auto it = S->templ.find(key);
+  if (it != S->templ.end()) return it->second.get();
+  // two contiguous transforms: the batch level of the lines is level 0 with
+  // stride n, which the descriptors rewrite per request
+  int64_t dims[2] = {n, 2}, st[2] = {1, n};
+  std::vector<int> reg{0};
+  fb_plan_s* P = create_plan(dtype, dir, 2, dims, st, st, reg, FB_DEFAULT_BLUESTEIN_CUTOFF,
+                             FB_FLAG_GENERIC_ONLY);
+  S->templ[key].reset(P);
+  return P;
+}
+
+static bool srv_single_pass(const fb_plan_s* P) {
+  return P->axes.size() == 1 && P->axes[0].passes.size() == 1 && P->axes[0].outer.empty() &&
+         P->axes[0].passes[0].a.ld.mode == 0 && P->axes[0].passes[0].a.st.mode == 0;
+}
+
+static fb_plan_s* srv_multi(fb_server_s* S, int64_t n, int dtype, int dir, int64_t batch) {
+  auto key = std::make_tuple(n, dtype, dir, batch);
+  auto it = S->multi.find(key);
+  if (it != S->multi.end()) return it->second.get();
+  int64_t dims[2] = {n, batch}, st[2] = {1, n};
+  std::vector<int> reg{0};
+  fb_plan_s* P = create_plan(dtype, dir, 2, dims, st, st, reg, FB_DEFAULT_BLUESTEIN_CUTOFF, 0);
+  S->multi[key].reset(P);
+  return P;
+}
+
+static size_t plan_scratch_bytes(const fb_plan_s* P) {
+  size_t b = 0;
+  if (P->scratch0) b += P->scratch0->bytes;
+  if (P->scratch1) b += P->scratch1->bytes;
+  return b;
+}
+
+static void srv_retire(fb_server_s* S, bool block) {
+  while (!S->inflight.empty()) {
+    bool done_any = false;
+    for (auto it = S->inflight.begin(); it != S->inflight.end();) {
+      cudaError_t q = block ? cudaEventSynchronize(it->ev) : cudaEventQuery(it->ev);
+      if (q == cudaErrorNotReady) {
+        ++it;
+        continue;
+      }
+      cuda_check(q, "server launch");
+      float ms = 0;
+      cuda_check(cudaEventElapsedTime(&ms, S->start, it->ev), "event time");
+      for (int64_t t : it->tickets) S->done.push_back({t, (double)ms});
+      S->admitted -= it->bytes;
+      cudaEventDestroy(it->ev);
+      it = S->inflight.erase(it);
+      done_any = true;
+    }
+    if (!block || !done_any) break;
+  }
+}
+
+// Shared-memory classes of descriptor launches (bytes per block).
+static const size_t kSmemClass[4] = {16u << 10, 48u << 10, 100u << 10, 220u << 10};
+
+static void srv_dispatch(fb_server_s* S) {
+  std::vector<SrvReq> batch;
+  while (!S->pending.empty()) {
+    const SrvReq& r = S->pending.front();
+    if (S->admitted + r.bytes > S->budget && (S->admitted > 0 || !batch.empty())) break;
+    S->admitted += r.bytes;
+    batch.push_back(r);
+    S->pending.pop_front();
+  }
+  S->st_max_admitted = std::max(S->st_max_admitted, S->admitted);
+  if (batch.empty()) return;
+  // groups of descriptors keyed by (dtype, variant, threads, smem class)
+  struct Group {
+    std::vector<LineArgs> descs;
+    std::vector<int64_t> bstart{0};
+    std::vector<int64_t> tickets;
+    double bytes = 0;
+    size_t smem = 0;
+  };
+  std::map<std::tuple<int, int, int, int>, Group> groups;
+  for (const SrvReq& r : batch) {
+    fb_plan_s* T = srv_template(S, r.n, r.dtype, r.dir);
+    if (!srv_single_pass(T)) {
+      fb_plan_s* P = srv_multi(S, r.n, r.dtype, r.dir, r.batch);
+      execute_plan(P, r.in, r.out, S->serial);
+      SrvLaunch l;
+      cuda_check(cudaEventCreateWithFlags(&l.ev, cudaEventDefault), "event");
+      cuda_check(cudaEventRecord(l.ev, S->serial), "event record");
+      l.tickets.push_back(r.ticket);
+      l.bytes = r.bytes;
+      l.slot = -1;
+      S->inflight.push_back(std::move(l));
+      S->st_launches += 1;
+      continue;
+    }
+    const Pass& p = T->axes[0].passes[0];
+    LineArgs a = p.a;
+    int Tt = a.T, var = p.variant;
+    std::vector<int> rad(a.prog.radix, a.prog.radix + a.prog.nst);
+    if (!pick_threads(a.prog.L, rad, &Tt, &var)) fail(FB_ERR_UNSUPPORTED, "no thread shape");
+    const int threads = Tt > 256 ? 512 : 256;
+    const size_t es = elem_bytes(r.dtype);
+    const size_t line_bytes = (size_t)a.Lpad * es + 4 * sizeof(int64_t);
+    int cls = 0;
+    while (cls < 3 && line_bytes > kSmemClass[cls]) ++cls;
+    int G = std::max(1, threads / Tt);
+    while (G > 1 && (size_t)G * line_bytes > kSmemClass[cls]) --G;
+    while (G > 1 && G / 2 >= r.batch) G /= 2;
+    a.T = Tt;
+    a.G = G;
+    a.in = r.in;
+    a.out = r.out;
+    a.nlines = r.batch;
+    a.m0 = r.batch;
+    a.m1 = 1;
+    a.scale = 1.0;
+    Group& g = groups[std::make_tuple(r.dtype, var, threads, cls)];
+    g.descs.push_back(a);
+    g.bstart.push_back(g.bstart.back() + (r.batch + G - 1) / G);
+    g.tickets.push_back(r.ticket);
+    g.bytes += r.bytes;
+    g.smem = std::max(g.smem, line_smem_bytes(r.dtype, a));
+  }
+  for (auto& kv : groups) {
+    Group& g = kv.second;
+    const int dtype = std::get<0>(kv.first), var = std::get<1>(kv.first);
+    const int threads = std::get<2>(kv.first);
+    const int nd = (int)g.descs.size();
+    // descriptor slot (reused once its previous launch has finished)
+    const int si = S->next_slot++ % (int)S->slots.size();
+    SrvSlot& slot = S->slots[si];
+    if (slot.last) {
+      cuda_check(cudaEventSynchronize(slot.last), "slot reuse");
+      cudaEventDestroy(slot.last);
+      slot.last = nullptr;
+    }
+    const size_t bytes = nd * sizeof(LineArgs) + (nd + 1) * sizeof(int64_t);
+    if (!slot.buf || slot.buf->bytes < bytes) slot.buf.reset(new DevBuf(bytes * 2));
+    if (slot.host_bytes < bytes) {
+      if (slot.host) cudaFreeHost(slot.host);
+      slot.host = nullptr;
+      slot.host_bytes = 0;
+      cuda_check(cudaMallocHost(&slot.host, bytes * 2), "pinned staging");
+      slot.host_bytes = bytes * 2;
+    }
+    unsigned char* host = (unsigned char*)slot.host;
+    memcpy(host, g.descs.data(), nd * sizeof(LineArgs));
+    memcpy(host + nd * sizeof(LineArgs), g.bstart.data(), (nd + 1) * sizeof(int64_t));
+    cudaStream_t st = S->streams[S->next_stream++ % S->streams.size()];
+    cuda_check(cudaMemcpyAsync(slot.buf->p, host, bytes, cudaMemcpyHostToDevice, st),
+               "descriptor copy");
+    const LineArgs* dd = (const LineArgs*)slot.buf->p;
+    const int64_t* db = (const int64_t*)((char*)slot.buf->p + nd * sizeof(LineArgs));
+    cuda_check(launch_desc(dtype, var, dd, db, nd, g.bstart.back(), threads, g.smem, st),
+               "descriptor launch");
+    SrvLaunch l;
+    cuda_check(cudaEventCreateWithFlags(&l.ev, cudaEventDefault), "event");
+    cuda_check(cudaEventRecord(l.ev, st), "event record");
+    cuda_check(cudaEventCreateWithFlags(&slot.last, cudaEventDisableTiming), "event");
+    cuda_check(cudaEventRecord(slot.last, st), "event record");
+    l.tickets = std::move(g.tickets);
+    l.bytes = g.bytes;
+    l.slot = si;
+    S->inflight.push_back(std::move(l));
+    S->st_launches += 1;
+    S->st_desc_launches += 1;
+  }
+}
+
+}  // namespace fb
+
+extern "C" {
+
+int fb_server_create(fb_server* srv, double budget_bytes, int nstreams, uint32_t flags) {
+  (void)flags;
+  return guard([&] {
+    if (!srv) fail(FB_ERR_ARGUMENT, "null argument");
+    *srv = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      fail(FB_ERR_CUDA, "no CUDA device: this library has no CPU fallback");
+    }
+    std::unique_ptr<fb_server_s> S(new fb_server_s());
+    cuda_check(cudaGetDevice(&S->device), "cudaGetDevice");
+    S->budget = budget_bytes > 0 ? budget_bytes : 100e9;
+    const int ns = std::max(1, std::min(nstreams, 16));
+    for (int i = 0; i < ns; ++i) {
+      cudaStream_t st;
+      cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+      S->streams.push_back(st);
+    }
+    cuda_check(cudaStreamCreateWithFlags(&S->serial, cudaStreamNonBlocking), "stream");
+    S->slots.resize(4 * ns);
+    cuda_check(cudaEventCreate(&S->start), "event");
+    cuda_check(cudaEventRecord(S->start, S->streams[0]), "event record");
+    cuda_check(cudaEventSynchronize(S->start), "event sync");
+    *srv = S.release();
+  });
+}
+
+int fb_server_submit(fb_server srv, int64_t n, int dtype, int dir, int64_t batch, const void* in,
+                     void* out, int64_t* ticket) {
+  return guard([&] {
+    if (!srv || !ticket) fail(FB_ERR_ARGUMENT, "null argument");
+    if (n <= 0) fail(FB_ERR_DIMENSION_MISMATCH, "Array length must be strictly positive");
+    if (dtype != FB_C32 && dtype != FB_C64)
+      fail(FB_ERR_ARGUMENT, "element type must be ComplexF32 or ComplexF64");
+    if (dir != FB_FORWARD && dir != FB_BACKWARD) fail(FB_ERR_ARGUMENT, "direction must be -1 or +1");
+    if (batch < 1 || !in || !out) fail(FB_ERR_ARGUMENT, "bad batch or data pointer");
+    // plans are made at submission (tables resident); bytes = data + scratch
+    fb_plan_s* T = srv_template(srv, n, dtype, dir);
+    double bytes = 2.0 * (double)n * (double)batch * elem_bytes(dtype);
+    if (!srv_single_pass(T)) bytes += (double)plan_scratch_bytes(srv_multi(srv, n, dtype, dir, batch));
+    SrvReq r{srv->next_ticket++, n, batch, dtype, dir, in, out, bytes};
+    srv->pending.push_back(r);
+    srv->st_requests += 1;
+    srv->st_max_queue = std::max<int64_t>(srv->st_max_queue, (int64_t)srv->pending.size());
+    *ticket = r.ticket;
+  });
+}
+
+int fb_server_submit_many(fb_server srv, int64_t count, const int64_t* n, const int32_t* dtype,
+                          const int32_t* dir, const int64_t* batch, const void* const* in,
+                          void* const* out, int64_t* tickets) {
+  for (int64_t i = 0; i < count; ++i) {
+    const int rc = fb_server_submit(srv, n[i], dtype[i], dir[i], batch[i], in[i], out[i],
+                                    tickets + i);
+    if (rc != FB_OK) return rc;
+  }
+  return FB_OK;
+}
+
+int fb_server_poll(fb_server srv, int64_t max, int64_t* tickets, double* done_ms, int64_t* count) {
+  return guard([&] {
+    if (!srv || !count) fail(FB_ERR_ARGUMENT, "null argument");
+    srv_retire(srv, false);
+    // keep at most one launch per stream (plus multi-pass work) in flight:
+    // whatever arrived meanwhile goes out together in the next dispatch
+    if ((int64_t)srv->inflight.size() < (int64_t)srv->streams.size()) srv_dispatch(srv);
+    int64_t k = 0;
+    while (k < max && !srv->done.empty()) {
+      tickets[k] = srv->done.front().first;
+      done_ms[k] = srv->done.front().second;
+      srv->done.erase(srv->done.begin());
+      ++k;
+    }
+    *count = k;
+  });
+}
+
+int fb_server_wait(fb_server srv) {
+  return guard([&] {
+    if (!srv) fail(FB_ERR_ARGUMENT, "null argument");
+    while (!srv->pending.empty() || !srv->inflight.empty()) {
+      srv_dispatch(srv);
+      srv_retire(srv, true);
+    }
+  });
+}
+
+int fb_server_stats(fb_server srv, int64_t* out, int nout) {
+  return guard([&] {
+    if (!srv || !out) fail(FB_ERR_ARGUMENT, "null argument");
+    const int64_t v[6] = {srv->st_requests, srv->st_launches, srv->st_desc_launches,
+                          srv->st_max_queue, (int64_t)srv->st_max_admitted,
+                          (int64_t)(srv->templ.size() + srv->multi.size())};
+    for (int i = 0; i < nout && i < 6; ++i) out[i] = v[i];
+  });
+}
+
+int fb_server_reset_clock(fb_server srv) {
+  return guard([&] {
+    if (!srv) fail(FB_ERR_ARGUMENT, "null argument");
+    cuda_check(cudaEventRecord(srv->start, srv->streams[0]), "event record");
+    cuda_check(cudaEventSynchronize(srv->start), "event sync");
+  });
+}
+
+int fb_server_destroy(fb_server srv) {
+  return guard([&] {
+    if (!srv) return;
+    cudaDeviceSynchronize();
+    delete srv;
+  });
+}
 
 }  // extern "C"

@@ -313,6 +313,7 @@ def _make_plan(x, region, direction, cutoff, scale_inverse=False, flags=0):
 
 
 FB_FLAG_GENERIC_ONLY = 1  # include/fftab200.h: generic kernels only (for tests)
+FB_FLAG_SAME_SCHEDULE_STRIDED = 2  # strided axes bit-identical to contiguous ones
 
 
 def plan_fft(x, region=None, *, BLUESTEIN_CUTOFF=DEFAULT_BLUESTEIN_CUTOFF, _flags=0, **_kwargs):

@@ -1,0 +1,389 @@
+"""Continuous-batching transform server over the sm_100a library.
+
+FFTA.jl has no serving layer; this module is the request loop the north star
+asks for on top of the drop-in path.  Requests are (length n, element type,
+direction, batch count, seed, arrival time).  The loop:
+
+* admits waiting requests in arrival order while their device bytes (input +
+  output + multi-pass scratch) fit a budget (100 GB by default), and releases
+  a request's bytes when it completes;
+* keeps plans (twiddle/chirp tables, scratch) resident, keyed by
+  (n, type, direction) -- and the batch for multi-pass lengths;
+* packs every admitted single-pass request -- any mix of lengths, types and
+  directions -- into one work-descriptor launch per kernel variant (each
+  block looks up its request's descriptor); multi-pass lengths run their
+  cached plans on a dedicated stream;
+* rotates launches over several CUDA streams and dispatches whatever arrived
+  while earlier launches run, as soon as a stream is free (continuous
+  batching); completions are timed with CUDA events on the device clock.
+
+The loop itself is native (fb_server_* in the C ABI); `Server` here drives it
+with arrivals and polls.
+
+`run_one_by_one` is the plain path it is compared with: each request, on
+arrival, runs its own plan and is synchronised before the next one starts.
+
+Both paths read the same device-resident inputs (generated from the
+per-request seeds before timing) so that what is compared is the serving of
+transforms, not data generation.
+"""
+from __future__ import annotations
+
+import collections
+import ctypes
+import dataclasses
+import math
+import time
+
+import numpy as np
+
+from . import _lib, _check, plan_fft, plan_bfft
+
+ELEM = {"c64": 8, "c128": 16}
+
+
+@dataclasses.dataclass
+class Request:
+    rid: int
+    n: int
+    kind: str  # "c64" (ComplexF32) or "c128" (ComplexF64)
+    dir: int  # -1 forward, +1 backward
+    batch: int
+    seed: int
+    arrival: float  # seconds from the start of the run
+    done: float = math.nan  # completion time, seconds from the start
+
+    @property
+    def bytes_io(self) -> int:
+        return 2 * self.n * self.batch * ELEM[self.kind]
+
+    @property
+    def flops(self) -> float:
+        return 5.0 * self.n * math.log2(max(self.n, 2)) * self.batch
+
+
+# ----------------------------------------------------------------- traces
+def _is_prime(v: int) -> bool:
+    if v < 2:
+        return False
+    if v % 2 == 0:
+        return v == 2
+    f = 3
+    while f * f <= v:
+        if v % f == 0:
+            return False
+        f += 2
+    return True
+
+
+def _smooth_near(target: float, primes, need=None) -> int:
+    """The product of `primes` closest to target (log scale), using `need`."""
+    best, bestd = 1, float("inf")
+    lt = math.log(target)
+
+    def rec(i, v):
+        nonlocal best, bestd
+        if v > target * 2:
+            return
+        if i == len(primes):
+            if need is not None and v % need:
+                return
+            d = abs(math.log(v) - lt)
+            if d < bestd:
+                best, bestd = v, d
+            return
+        p = primes[i]
+        while v <= target * 2:
+            rec(i + 1, v)
+            v *= p
+
+    rec(0, 1)
+    return best
+
+
+def make_trace(count: int, rate: float, seed: int = 0, n_min: int = 64, n_max: int = 2 ** 20,
+               batch_max: int = 512, mix=(0.5, 0.2, 0.15, 0.15), c64_frac=0.2):
+    """Requests of the serving configuration.
+
+    Length log-uniform on [n_min, n_max] and rounded into its class: 50 % powers
+    of two, 20 % 2^a 3^b (b >= 1), 15 % other smooth composites (a factor 5 or
+    7), 15 % primes; direction forward/backward 50/50; ComplexF32 80 % /
+    ComplexF64 20 %; batch uniform on 1..batch_max; Poisson arrivals at `rate`
+    requests per second; one seed per request.
+    """
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    lo, hi = math.log(n_min), math.log(n_max)
+    for i in range(count):
+        t += rng.exponential(1.0 / rate) if rate > 0 else 0.0
+        target = math.exp(rng.uniform(lo, hi))
+        c = rng.choice(4, p=list(mix))
+        if c == 0:
+            n = 2 ** int(round(math.log2(target)))
+        elif c == 1:
+            n = _smooth_near(target, [2, 3], need=3)
+        elif c == 2:
+            n = _smooth_near(target, [2, 3, 5, 7], need=int(rng.choice([5, 7])))
+        else:
+            n = int(target)
+            while not _is_prime(n):
+                n += 1
+        n = int(min(max(n, n_min if c != 3 else 2), n_max * 2))
+        kind = "c128" if rng.random() < c64_frac else "c64"
+        out.append(Request(i, n, kind, -1 if rng.random() < 0.5 else 1,
+                           int(rng.integers(1, batch_max + 1)), int(rng.integers(0, 2 ** 31)), t))
+    return out
+
+
+def make_inputs(trace, device):
+    """Device-resident complex-normal inputs, one per request, from its seed."""
+    import torch
+    xs = []
+    for r in trace:
+        g = torch.Generator(device=device)
+        g.manual_seed(r.seed)
+        rdt = torch.float32 if r.kind == "c64" else torch.float64
+        shape = (r.batch, r.n)
+        xs.append(torch.complex(torch.randn(shape, generator=g, device=device, dtype=rdt),
+                                torch.randn(shape, generator=g, device=device, dtype=rdt)))
+    return xs
+
+
+# ------------------------------------------------------------------ plans
+class PlanCache:
+    """Resident plans: grouped (n, kind, dir) and per-batch (n, kind, dir, batch)."""
+
+    def __init__(self):
+        self.group = {}
+        self.single = {}
+
+    def _make(self, n, kind, direction, batch):
+        import torch
+        dt = torch.complex64 if kind == "c64" else torch.complex128
+        x = torch.empty((batch, n), dtype=dt, device="cuda")
+        p = (plan_fft if direction < 0 else plan_bfft)(x.T, 1)
+        p._cplan(x.T, x.T)  # build the device schedule now
+        return p, p._cplans[next(iter(p._cplans))]
+
+    def grouped(self, n, kind, direction):
+        key = (n, kind, direction)
+        if key not in self.group:
+            p, h = self._make(n, kind, direction, 1)
+            buf = ctypes.create_string_buffer(4096)
+            _check(_lib.lib.fb_plan_describe(h, buf, len(buf)))
+            ok = "FAST(" in buf.value.decode() and buf.value.decode().count("(") == 1
+            self.group[key] = (p, h, ok)
+        return self.group[key]
+
+    def single_plan(self, n, kind, direction, batch):
+        key = (n, kind, direction, batch)
+        if key not in self.single:
+            self.single[key] = self._make(n, kind, direction, batch)
+        return self.single[key]
+
+    def scratch_bytes(self, r: Request) -> int:
+        p, h = self.single_plan(r.n, r.kind, r.dir, r.batch) if not self.grouped(
+            r.n, r.kind, r.dir)[2] else self.grouped(r.n, r.kind, r.dir)[:2]
+        v = ctypes.c_size_t()
+        _check(_lib.lib.fb_plan_device_bytes(h, ctypes.byref(v)))
+        return int(v.value)
+
+
+def warm_plans(trace, cache: PlanCache):
+    for r in trace:
+        _, _, ok = cache.grouped(r.n, r.kind, r.dir)
+        if not ok:
+            cache.single_plan(r.n, r.kind, r.dir, r.batch)
+
+
+# ------------------------------------------------------------- execution
+def _stream_ptr(s):
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _run_single(cache, r, x, y, stream):
+    _, h, ok = cache.grouped(r.n, r.kind, r.dir)
+    if ok:
+        ins = (ctypes.c_void_p * 1)(x.data_ptr())
+        outs = (ctypes.c_void_p * 1)(y.data_ptr())
+        bs = (ctypes.c_int64 * 1)(r.batch)
+        _check(_lib.lib.fb_execute_grouped(h, 1, ins, outs, bs, _stream_ptr(stream)))
+    else:
+        _, hs = cache.single_plan(r.n, r.kind, r.dir, r.batch)
+        _check(_lib.lib.fb_execute(hs, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(y.data_ptr()),
+                                   _stream_ptr(stream)))
+
+
+def _stats(trace, wall, label):
+    lat = np.array([r.done - r.arrival for r in trace])
+    fl = sum(r.flops for r in trace)
+    by = sum(r.bytes_io for r in trace)
+    span = max(r.done for r in trace) - min(r.arrival for r in trace)
+    return {
+        "path": label, "requests": len(trace), "wall_s": wall, "span_s": span,
+        "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+        "mean_ms": float(lat.mean() * 1e3),
+        "throughput_req_s": len(trace) / span, "GFLOP/s": fl / span / 1e9, "GB/s": by / span / 1e9,
+    }
+
+
+def run_one_by_one(trace, xs, ys, cache: PlanCache):
+    """One launch per request, each synchronised before the next (the plain path)."""
+    import torch
+    stream = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for r, x, y in zip(trace, xs, ys):
+        now = time.perf_counter() - t0
+        if now < r.arrival:
+            time.sleep(r.arrival - now)
+        _run_single(cache, r, x, y, stream)
+        stream.synchronize()
+        r.done = time.perf_counter() - t0
+    return _stats(trace, time.perf_counter() - t0, "one_launch_per_request")
+
+
+class Server:
+    """Driver of the library's native server (fb_server_*): submits each
+    request when it arrives and polls for completions.  Admission, packing
+    into work-descriptor launches and stream rotation happen in the library.
+    Completion times come from CUDA events on the device clock, counted from
+    the server's creation (the run's time origin)."""
+
+    KIND = {"c64": _lib.FB_C32, "c128": _lib.FB_C64}
+
+    def __init__(self, budget_bytes: float = 100e9, nstreams: int = 4):
+        self.budget = budget_bytes
+        self.nstreams = nstreams
+        self.h = ctypes.c_void_p()
+        _check(_lib.lib.fb_server_create(ctypes.byref(self.h), float(budget_bytes), nstreams, 0))
+
+    def __del__(self):
+        try:
+            _lib.lib.fb_server_destroy(self.h)
+        except Exception:
+            pass
+
+    def run(self, trace, xs, ys):
+        """Serve `trace` (arrival times relative to the call); the server's
+        plans stay resident between runs."""
+        import torch
+        torch.cuda.synchronize()
+        h = self.h
+        st0 = (ctypes.c_int64 * 6)()
+        _check(_lib.lib.fb_server_stats(h, st0, 6))
+        n = len(trace)
+        # request fields as arrays, so that everything that has arrived is
+        # submitted with one call
+        a_n = np.array([r.n for r in trace], dtype=np.int64)
+        a_t = np.array([self.KIND[r.kind] for r in trace], dtype=np.int32)
+        a_d = np.array([r.dir for r in trace], dtype=np.int32)
+        a_b = np.array([r.batch for r in trace], dtype=np.int64)
+        a_in = (ctypes.c_void_p * n)(*[x.data_ptr() for x in xs[:n]])
+        a_out = (ctypes.c_void_p * n)(*[y.data_ptr() for y in ys[:n]])
+        tickets = np.zeros(n, dtype=np.int64)
+        arrivals = np.array([r.arrival for r in trace])
+        cap = 4096
+        tk = np.zeros(cap, dtype=np.int64)
+        tm = np.zeros(cap, dtype=np.float64)
+        cnt = ctypes.c_int64()
+        i64 = ctypes.POINTER(ctypes.c_int64)
+        i32 = ctypes.POINTER(ctypes.c_int32)
+        vpp = ctypes.POINTER(ctypes.c_void_p)
+        sz = ctypes.sizeof(ctypes.c_void_p)
+        done = np.full(n, np.nan)
+        base = None
+        _check(_lib.lib.fb_server_reset_clock(h))
+        t0 = time.perf_counter()
+        nxt, ndone = 0, 0
+        try:
+            while ndone < n:
+                now = time.perf_counter() - t0
+                upto = int(np.searchsorted(arrivals, now, side="right"))
+                if upto > nxt:
+                    k = upto - nxt
+                    _check(_lib.lib.fb_server_submit_many(
+                        h, k, a_n[nxt:].ctypes.data_as(i64), a_t[nxt:].ctypes.data_as(i32),
+                        a_d[nxt:].ctypes.data_as(i32), a_b[nxt:].ctypes.data_as(i64),
+                        ctypes.cast(ctypes.addressof(a_in) + nxt * sz, vpp),
+                        ctypes.cast(ctypes.addressof(a_out) + nxt * sz, vpp),
+                        tickets[nxt:].ctypes.data_as(i64)))
+                    if base is None:
+                        base = int(tickets[0])  # tickets are consecutive
+                    nxt = upto
+                _check(_lib.lib.fb_server_poll(h, cap, tk.ctypes.data_as(i64),
+                                               tm.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                               ctypes.byref(cnt)))
+                c = cnt.value
+                if c:
+                    done[tk[:c] - base] = tm[:c] * 1e-3
+                ndone += c
+                if cnt.value == 0 and nxt < n and ndone == nxt:
+                    dt = arrivals[nxt] - (time.perf_counter() - t0)
+                    if dt > 0:
+                        time.sleep(min(dt, 0.0005))
+        finally:
+            st6 = (ctypes.c_int64 * 6)()
+            _check(_lib.lib.fb_server_stats(h, st6, 6))
+        for r, d in zip(trace, done):
+            r.done = float(d)
+        out = _stats(trace, time.perf_counter() - t0, "continuous_batching")
+        out.update({"launches": st6[1] - st0[1], "descriptor_launches": st6[2] - st0[2],
+                    "max_queue": st6[3], "max_admitted_GB": st6[4] / 1e9,
+                    "resident_plans": st6[5], "streams": self.nstreams})
+        return out
+
+
+def check_mix_equals_alone(trace, xs, ys_mix, cache: PlanCache):
+    """Each request's result in the mix equals its result run alone (bitwise)."""
+    import torch
+    worst = 0.0
+    for r, x, y in zip(trace, xs, ys_mix):
+        alone = torch.empty_like(x)
+        _run_single(cache, r, x, alone, torch.cuda.current_stream())
+        torch.cuda.synchronize()
+        d = (alone - y).abs().max().item()
+        worst = max(worst, d)
+    return worst
+
+
+# ------------------------------------------------------------ benchmark
+def compare(count=400, rates=(2000.0,), seed=11, n_max=2 ** 20, batch_max=512,
+            max_elems=1 << 22, budget_bytes=100e9, nstreams=4):
+    """Serve one trace with both paths at each arrival rate of a sweep.
+
+    Requests whose n * batch exceeds `max_elems` get their batch reduced so the
+    whole trace's inputs fit on the device next to the outputs (the bounded
+    sample of the configuration; the distribution of n is unchanged).  Returns
+    {"sweep": [{rate, batched, one_launch_per_request}...], "notes": ...}.
+    """
+    import torch
+    base = make_trace(count, 1.0, seed, n_max=n_max, batch_max=batch_max)
+    capped = 0
+    for r in base:
+        if r.n * r.batch > max_elems:
+            r.batch = max(1, max_elems // r.n)
+            capped += 1
+    cache = PlanCache()
+    warm_plans(base, cache)
+    xs = make_inputs(base, "cuda")
+    ys = [torch.empty_like(x) for x in xs]
+    srv = Server(budget_bytes, nstreams)
+    srv.run([dataclasses.replace(r, arrival=0.0) for r in base], xs, ys)  # resident plans
+    run_one_by_one([dataclasses.replace(r, arrival=0.0) for r in base[:8]], xs[:8], ys[:8], cache)
+    worst = check_mix_equals_alone(base[:50], xs[:50], ys[:50], cache)
+    sweep = []
+    for rate in rates:
+        # the same requests, arrivals rescaled to `rate` (rate 0: all at once)
+        tr = [dataclasses.replace(r, arrival=(r.arrival / rate if rate > 0 else 0.0))
+              for r in base]
+        b = srv.run([dataclasses.replace(r) for r in tr], xs, ys)
+        p = run_one_by_one([dataclasses.replace(r) for r in tr], xs, ys, cache)
+        sweep.append({"rate_req_s": rate if rate > 0 else "all_at_t0", "batched": b,
+                      "one_launch_per_request": p,
+                      "throughput_ratio": b["throughput_req_s"] / p["throughput_req_s"]})
+    notes = {"requests": count, "requests_with_batch_capped": capped,
+             "max_elems_per_request": max_elems, "mix_vs_alone_max_abs_diff": worst,
+             "distinct_plans": len(cache.group) + len(cache.single)}
+    return {"sweep": sweep, "notes": notes}

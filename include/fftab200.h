@@ -44,10 +44,18 @@ enum { FB_C32 = 0, FB_C64 = 1 };          /* ComplexF32, ComplexF64 */
 enum { FB_FORWARD = -1, FB_BACKWARD = 1 };
 enum { FB_DEFAULT_BLUESTEIN_CUTOFF = 73 }; /* src/callgraph.jl:44 */
 
-/* Plan flags.  FB_FLAG_GENERIC_ONLY: use only the generic line kernel, never
- * the length-specialised ones (results are bit-identical either way; the
- * flag exists so tests can check that). */
-enum { FB_FLAG_GENERIC_ONLY = 1u };
+/* Plan flags.
+ * FB_FLAG_GENERIC_ONLY: use only the generic line kernel, never the
+ *   length-specialised ones (results are bit-identical either way; the flag
+ *   exists so tests can check that).
+ * FB_FLAG_SAME_SCHEDULE_STRIDED: transform long strided lines (longer than
+ *   about 750 elements, e.g. the columns of a large 2-D array) with the
+ *   schedule of a contiguous line of that length.  By default such axes use a
+ *   four-step split that moves long contiguous runs; its results equal the
+ *   contiguous schedule's within rounding but not bit for bit.  With the flag
+ *   every strided transform is bit-identical to the same transform of a
+ *   contiguous copy (FFTA's `==` property), at lower speed for those axes. */
+enum { FB_FLAG_GENERIC_ONLY = 1u, FB_FLAG_SAME_SCHEDULE_STRIDED = 2u };
 
 /* Batched 1-D plan: `batch` transforms of length n; element j of transform b
  * is read at in[b*idist + j*istride] and written at out[b*odist + j*ostride].
@@ -92,6 +100,50 @@ int fb_execute(fb_plan plan, const void* in, void* out, void* stream);
  * when `out` holds the result.  Pinned host memory gives full copy speed.
  * Replaces Base.:*(p, x) on a CPU array (src/plan.jl:374-384). */
 int fb_execute_host(fb_plan plan, const void* in, void* out, void* stream);
+
+/* Run one batched 1-D plan over `count` requests in a single kernel launch:
+ * request r has batches[r] contiguous transforms of the plan's length n at
+ * device pointers ins[r] / outs[r] (distance n; the plan's own batch count is
+ * ignored).  The descriptor table is copied to the device on `stream`; calls
+ * with the same plan must stay on one stream.  Only plans whose length runs
+ * in one specialised pass support this (else FB_ERR_UNSUPPORTED).  No FFTA
+ * counterpart: FFTA runs each call's columns serially (src/plan.jl:204-206);
+ * this is the work-descriptor launch of the serving loop. */
+int fb_execute_grouped(fb_plan plan, int64_t count, const void* const* ins, void* const* outs,
+                       const int64_t* batches, void* stream);
+
+/* Serving: continuous batching over work-descriptor launches.  No FFTA
+ * counterpart (FFTA is a library of synchronous calls).  A server admits
+ * requests in arrival order while their device bytes (input + output + any
+ * multi-pass scratch) fit `budget_bytes`, packs all admitted single-pass
+ * requests -- any mix of lengths, types and directions -- into one kernel
+ * launch per kernel variant, runs multi-pass lengths with cached plans on a
+ * dedicated stream, and rotates launches over `nstreams` CUDA streams. */
+typedef struct fb_server_s* fb_server;
+int fb_server_create(fb_server* srv, double budget_bytes, int nstreams, uint32_t flags);
+/* Queue `batch` contiguous transforms of length n (device pointers; the
+ * caller keeps them alive until the ticket completes).  Nothing is launched
+ * until fb_server_poll / fb_server_wait. */
+int fb_server_submit(fb_server srv, int64_t n, int dtype, int dir, int64_t batch, const void* in,
+                     void* out, int64_t* ticket);
+/* fb_server_submit for `count` requests given as arrays (one call for every
+ * request that arrived since the last poll); stops at the first error. */
+int fb_server_submit_many(fb_server srv, int64_t count, const int64_t* n, const int32_t* dtype,
+                          const int32_t* dir, const int64_t* batch, const void* const* in,
+                          void* const* out, int64_t* tickets);
+/* Retire finished launches, dispatch what is queued when a stream is free,
+ * and return up to `max` completed tickets with their completion times (ms
+ * on the device clock since fb_server_create). */
+int fb_server_poll(fb_server srv, int64_t max, int64_t* tickets, double* done_ms, int64_t* count);
+/* Dispatch and wait until every submitted request has completed. */
+int fb_server_wait(fb_server srv);
+/* out[0..5]: requests, launches, descriptor launches, max queue depth, max
+ * admitted bytes, resident plans. */
+int fb_server_stats(fb_server srv, int64_t* out, int nout);
+/* Restart the clock of fb_server_poll's completion times (waits until the
+ * server's first stream is idle). */
+int fb_server_reset_clock(fb_server srv);
+int fb_server_destroy(fb_server srv);
 
 /* Base.size(p, i) (src/plan.jl:36-47): the transform length along the i-th
  * region entry, 1 past the last one, FB_ERR_DOMAIN for i < 1. */

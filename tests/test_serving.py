@@ -1,0 +1,66 @@
+"""Serving loop: trace generation (host) and, on the GPU, continuous batching.
+
+The GPU tests check that every request's result is the same when it runs in
+the mix (grouped launches, several streams, admission under a budget) as when
+it runs alone, and that results match the oracle within the parity tolerance.
+"""
+import numpy as np
+import pytest
+
+from ffta_b200 import serving
+
+
+def test_trace_distribution():
+    tr = serving.make_trace(4000, rate=1000.0, seed=3)
+    ns = np.array([r.n for r in tr])
+    assert ns.min() >= 2 and ns.max() <= 2 ** 21
+    pow2 = np.mean([(n & (n - 1)) == 0 for n in ns])
+    assert 0.42 < pow2 < 0.58
+    primes = np.mean([serving._is_prime(int(n)) for n in ns])
+    assert 0.1 < primes < 0.2
+    c64 = np.mean([r.kind == "c128" for r in tr])
+    assert 0.15 < c64 < 0.25
+    assert all(1 <= r.batch <= 512 for r in tr)
+    arr = np.array([r.arrival for r in tr])
+    assert np.all(np.diff(arr) >= 0)
+    assert abs(len(tr) / arr[-1] - 1000.0) < 100.0
+
+
+@pytest.mark.gpu
+def test_mix_equals_alone_and_oracle():
+    import torch
+    import oracle
+    tr = serving.make_trace(60, rate=2000.0, seed=5, n_max=2 ** 14, batch_max=8)
+    xs = serving.make_inputs(tr, "cuda")
+    ys = [torch.empty_like(x) for x in xs]
+    cache = serving.PlanCache()
+    serving.warm_plans(tr, cache)
+    srv = serving.Server(budget_bytes=64 << 20, nstreams=3)
+    st = srv.run(tr, xs, ys)
+    assert st["requests"] == len(tr) and st["launches"] <= len(tr)
+    assert serving.check_mix_equals_alone(tr, xs, ys, cache) == 0.0
+    for r, x, y in list(zip(tr, xs, ys))[:20]:
+        ref = oracle.fft_nd(x.cpu().numpy().T, 1, r.dir, prec="f64").T
+        eps = 2.0 ** -23 if r.kind == "c64" else 2.0 ** -52
+        err = np.linalg.norm(y.cpu().numpy() - ref) / np.linalg.norm(ref)
+        assert err <= 4 * eps * max(1.0, np.log2(r.n)), (r, err)
+
+
+@pytest.mark.gpu
+def test_one_launch_for_mixed_requests():
+    """Requests of different lengths, types and directions that are queued
+    together go out as one descriptor launch per kernel variant, and each
+    result equals the same transform run alone through its own plan."""
+    import torch
+    import ffta_b200 as F
+    spec = [(4096, "c64", -1, 1), (1000, "c64", 1, 3), (4096, "c64", 1, 7), (243, "c64", -1, 2),
+            (97, "c64", -1, 5), (2048, "c128", -1, 2), (35, "c128", 1, 4)]
+    reqs = [serving.Request(i, n, k, d, b, i, 0.0) for i, (n, k, d, b) in enumerate(spec)]
+    xs = serving.make_inputs(reqs, "cuda")
+    ys = [torch.empty_like(x) for x in xs]
+    st = serving.Server(nstreams=2).run(reqs, xs, ys)
+    # one launch per (type, kernel variant, shared-memory class): 2 for C32, 2 for C64
+    assert st["descriptor_launches"] <= 4 and st["launches"] == st["descriptor_launches"]
+    for r, x, y in zip(reqs, xs, ys):
+        f = F.fft if r.dir < 0 else F.bfft
+        assert torch.equal(y, f(x.T, 1).T), r
