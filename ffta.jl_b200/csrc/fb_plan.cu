@@ -326,8 +326,9 @@ static void use_tile(const fb_plan_s* P, Pass& p, const std::vector<int>& radice
   const int thr_cap = std::max(1, std::max(512, T) / T);
   const int smem_cap = (int)std::max<size_t>(1, (100 * 1024) / ((size_t)ff->lpad * es));
   const bool em = p.a.ld.mode == 1 || p.a.st.mode == 1;
-  int want = std::max(1, 256 / T);
-  if (em) want = std::max(want, es == 8 ? 16 : 8);
+  // strided tiles: as many neighbouring lines as the block allows (longer
+  // contiguous runs per DRAM page); contiguous lines: 256-thread blocks
+  const int want = em ? thr_cap : std::max(1, 256 / T);
   int G = std::min(std::min(thr_cap, smem_cap), want);
   const int64_t nl = std::max<int64_t>(1, p.a.nlines);
   while (G > 1 && G / 2 >= nl) G /= 2;
