@@ -209,12 +209,10 @@ def main():
         if world > 1:
             dist.barrier()
 
+    from ffta_b200 import sharding
+
     def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return sharding.max_over_ranks(v, dev)
 
     g = torch.Generator(device=dev)
     g.manual_seed(1234 + rank)

@@ -305,6 +305,20 @@ struct fb_plan_s {
   std::unique_ptr<fb::DevBuf> hin, hout;
   // grouped execution: device copy of the request descriptors
   std::unique_ptr<fb::DevBuf> desc;
+  // pipelined host execution: plans for one chunk and the last one, device
+  // slots, streams and events
+  std::unique_ptr<fb_plan_s> chunk_plan, tail_plan;
+  int64_t chunk = 0;
+  std::vector<std::unique_ptr<fb::DevBuf>> slots;
+  cudaStream_t pstream[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t pev[3][3] = {};
+  ~fb_plan_s() {
+    for (auto s : pstream)
+      if (s) cudaStreamDestroy(s);
+    for (auto& row : pev)
+      for (auto e : row)
+        if (e) cudaEventDestroy(e);
+  }
   int64_t in_span = 0, out_span = 0;
   size_t table_bytes = 0;
 };
@@ -1077,10 +1091,71 @@ int fb_execute(fb_plan plan, const void* in, void* out, void* stream) {
   });
 }
 
+// Pipelined host execution of a batched 1-D plan over contiguous columns:
+// the batch is cut into chunks of about kHostChunk bytes that rotate through
+// three device slots; each chunk is copied in on one stream, transformed in
+// place on a second and copied out on a third, so the two copy directions and
+// the kernels overlap.  Returns false when the plan is not of that shape.
+static const size_t kHostChunk = 32u << 20;
+
+static bool host_pipeline(fb_plan_s* P, const void* in, void* out) {
+  if (P->rank != 2 || P->region.size() != 1 || P->region[0] != 0) return false;
+  const int64_t n = P->dims[0], B = P->dims[1];
+  if (P->istrides[0] != 1 || P->ostrides[0] != 1 || P->istrides[1] != n || P->ostrides[1] != n)
+    return false;
+  const size_t es = elem_bytes(P->dtype);
+  const size_t col = (size_t)n * es;
+  if ((size_t)B * col <= 2 * kHostChunk || col > kHostChunk) return false;
+  if (!P->chunk_plan) {
+    const int64_t chunk = std::max<int64_t>(1, (int64_t)(kHostChunk / col));
+    int64_t dims[2] = {n, chunk}, st[2] = {1, n};
+    std::vector<int> reg{0};
+    P->chunk_plan.reset(create_plan(P->dtype, P->dir, 2, dims, st, st, reg, P->cutoff, P->flags));
+    P->chunk_plan->scale = P->scale;
+    if (B % chunk) {
+      int64_t dt[2] = {n, B % chunk};
+      P->tail_plan.reset(create_plan(P->dtype, P->dir, 2, dt, st, st, reg, P->cutoff, P->flags));
+      P->tail_plan->scale = P->scale;
+    }
+    P->chunk = chunk;
+    for (int i = 0; i < 3; ++i) {
+      P->slots.emplace_back(new DevBuf((size_t)chunk * col));
+      cuda_check(cudaStreamCreateWithFlags(&P->pstream[i], cudaStreamNonBlocking), "stream");
+      for (int j = 0; j < 3; ++j)
+        cuda_check(cudaEventCreateWithFlags(&P->pev[i][j], cudaEventDisableTiming), "event");
+    }
+  }
+  P->chunk_plan->scale = P->scale;
+  if (P->tail_plan) P->tail_plan->scale = P->scale;
+  const int64_t chunk = P->chunk, nch = (B + chunk - 1) / chunk;
+  cudaStream_t h2d = P->pstream[0], comp = P->pstream[1], d2h = P->pstream[2];
+  for (int64_t c = 0; c < nch; ++c) {
+    const int k = (int)(c % 3);
+    const int64_t cols = std::min(chunk, B - c * chunk);
+    const size_t bytes = (size_t)cols * col;
+    void* slot = P->slots[k]->p;
+    // the slot is free once its previous chunk has been copied out
+    if (c >= 3) cuda_check(cudaStreamWaitEvent(h2d, P->pev[k][2], 0), "wait");
+    cuda_check(cudaMemcpyAsync(slot, (const char*)in + (size_t)c * chunk * col, bytes,
+                               cudaMemcpyHostToDevice, h2d), "copy in");
+    cuda_check(cudaEventRecord(P->pev[k][0], h2d), "event");
+    cuda_check(cudaStreamWaitEvent(comp, P->pev[k][0], 0), "wait");
+    execute_plan(cols == chunk ? P->chunk_plan.get() : P->tail_plan.get(), slot, slot, comp);
+    cuda_check(cudaEventRecord(P->pev[k][1], comp), "event");
+    cuda_check(cudaStreamWaitEvent(d2h, P->pev[k][1], 0), "wait");
+    cuda_check(cudaMemcpyAsync((char*)out + (size_t)c * chunk * col, slot, bytes,
+                               cudaMemcpyDeviceToHost, d2h), "copy out");
+    cuda_check(cudaEventRecord(P->pev[k][2], d2h), "event");
+  }
+  cuda_check(cudaStreamSynchronize(d2h), "synchronize");
+  return true;
+}
+
 int fb_execute_host(fb_plan plan, const void* in, void* out, void* stream) {
   return guard([&] {
     if (!plan) fail(FB_ERR_ARGUMENT, "null plan");
     if (plan->in_span == 0) return;
+    if (host_pipeline(plan, in, out)) return;
     const int es = elem_bytes(plan->dtype);
     const size_t ib = (size_t)plan->in_span * es, ob = (size_t)plan->out_span * es;
     if (!plan->hin || plan->hin->bytes < ib) plan->hin.reset(new DevBuf(ib));

@@ -297,6 +297,19 @@ def test_bluestein_cutoff_kwarg(cut):
         assert relerr(F.fft(x, BLUESTEIN_CUTOFF=cut), ref) <= tol(np.complex128, n)
 
 
+@pytest.mark.parametrize("n,B,dtype", [(4096, 2600, np.complex64), (1000, 5000, np.complex128)])
+def test_host_pipeline_matches_device(n, B, dtype):
+    """Host arrays above the chunk size go through the three-stream pipeline
+    (copy in / transform / copy out); results equal the device path bitwise."""
+    import torch
+    rng = np.random.default_rng(n)
+    x = crandn(rng, (B, n), dtype)
+    for planner in (F.plan_fft, F.plan_ifft):
+        host = planner(x.T, 1) * x.T
+        dev = (planner(x.T, 1) * torch.from_numpy(x).cuda().T).cpu().numpy()
+        assert np.array_equal(host, dev)
+
+
 def test_in_place_and_strided():
     import torch
     rng = np.random.default_rng(5)
