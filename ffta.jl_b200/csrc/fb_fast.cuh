@@ -93,11 +93,18 @@ template <typename R> struct TileIn {
   const cplx<R>* __restrict__ mul;
   int64_t vn, ves, voff;
   bool ok;
+  const cplx<R>* __restrict__ tab;  // twiddle on load (LineArgs::tw_on_load)
+  int64_t tab_es, tab_off;
+  int tw_dir;
   __device__ __forceinline__ cplx<R> operator()(int i) const {
     const int64_t vi = (int64_t)i * ves + voff;
     if (!ok || vi >= vn) return Sc<R>::mk(R(0), R(0));
     cplx<R> v = base[(int64_t)i * es];
     if (mul) v = cmul<R>(v, __ldg(mul + vi));
+    if (tab) {
+      const cplx<R> w = __ldg(tab + (int64_t)i * tab_es + tab_off);
+      v = tw_dir < 0 ? cmul<R>(v, w) : cmulc<R>(v, w);
+    }
     return v;
   }
 };
@@ -114,11 +121,16 @@ template <typename R> struct TileOut {
   int tw_shift, tw_dir;
   R scale;
   bool ok;
+  const cplx<R>* __restrict__ tab;  // full twiddle table (precedence over hi/lo)
+  int64_t tab_es, tab_off;
   __device__ __forceinline__ void operator()(int i, cplx<R> v) const {
     const int64_t vi = (int64_t)i * ves + voff;
     if (!ok || vi >= vn) return;
     if (mul) v = cmul<R>(v, __ldg(mul + vi));
-    if (tw_hi) {
+    if (tab) {
+      const cplx<R> w = __ldg(tab + (int64_t)i * tab_es + tab_off);
+      v = tw_dir < 0 ? cmul<R>(v, w) : cmulc<R>(v, w);
+    } else if (tw_hi) {
       const int64_t e = l0 * (int64_t)i;
       const cplx<R> w = cmul<R>(__ldg(tw_hi + (e >> tw_shift)),
                                 __ldg(tw_lo + (e & ((int64_t(1) << tw_shift) - 1))));
@@ -126,6 +138,40 @@ template <typename R> struct TileOut {
     }
     if (scale != R(1)) v = cscale<R>(v, scale);
     base[(int64_t)i * es] = v;
+  }
+};
+
+// Lean I/O for the common case (LineArgs::plain_io): every element present,
+// no chirp tables, 32-bit strides, twiddle (if any) from a full table.  The
+// line index is clamped to a valid line, so loads need no predicate.
+template <typename R> struct PlainIn {
+  const cplx<R>* __restrict__ base;
+  int es;
+  const cplx<R>* __restrict__ tab;  // twiddle on load (LineArgs::tw_on_load)
+  int tab_es, tab_off, tw_dir;
+  __device__ __forceinline__ cplx<R> operator()(int i) const {
+    cplx<R> v = base[(int64_t)(i * es)];
+    if (tab) {
+      const cplx<R> w = __ldg(tab + (i * tab_es + tab_off));
+      v = tw_dir < 0 ? cmul<R>(v, w) : cmulc<R>(v, w);
+    }
+    return v;
+  }
+};
+template <typename R> struct PlainOut {
+  cplx<R>* __restrict__ base;
+  int es;
+  const cplx<R>* __restrict__ tab;
+  int tab_es, tab_off, tw_dir;
+  R scale;
+  bool ok;
+  __device__ __forceinline__ void operator()(int i, cplx<R> v) const {
+    if (tab) {
+      const cplx<R> w = __ldg(tab + (i * tab_es + tab_off));
+      v = tw_dir < 0 ? cmul<R>(v, w) : cmulc<R>(v, w);
+    }
+    if (scale != R(1)) v = cscale<R>(v, scale);
+    if (ok) base[(int64_t)(i * es)] = v;
   }
 };
 
@@ -237,7 +283,7 @@ __global__ void __launch_bounds__(DirectBounds<R, T>::threads, DirectBounds<R, T
 // levels, element strides, presence window, tables).  Thread (g, u) is
 // threadIdx.x = g, threadIdx.y = u, so a warp spans 32/G butterflies of G
 // lines.  MID: forward program, multiply by a.mid, inverse program.
-template <typename R, class RL, int T, bool MID>
+template <typename R, class RL, int T, bool MID, bool PLAIN>
 __global__ void __launch_bounds__(T > 512 ? T : 512) fast_tile_kernel(const LineArgs a) {
   typedef cplx<R> C;
   constexpr int L = prog_len<RL>();
@@ -245,32 +291,57 @@ __global__ void __launch_bounds__(T > 512 ? T : 512) fast_tile_kernel(const Line
   extern __shared__ __align__(16) unsigned char smraw[];
   const int g = threadIdx.x, u = threadIdx.y;
   C* buf = (C*)smraw + g * LPAD;
+  // one thread per line splits its index into the batch levels (64-bit
+  // divisions) and leaves the results in shared memory for the others
+  int64_t* lb = (int64_t*)((C*)smraw + (size_t)a.G * LPAD);
   const int64_t line = (int64_t)blockIdx.x * a.G + g;
   const bool ok = line < a.nlines;
-  const int64_t l = ok ? line : 0;
-  const int64_t l0 = l % a.m0, t = l / a.m0;
-  const int64_t l1 = t % a.m1, l2 = t / a.m1;
-  const TileIn<R> in{(const C*)a.in + (l0 * a.ld.s0 + l1 * a.ld.s1 + l2 * a.ld.s2), a.ld.es,
-                     (const C*)a.ld.mul, a.ld.vn, a.ld.ves, l0 * a.ld.vls, ok};
-  const TileOut<R> out{(C*)a.out + (l0 * a.st.s0 + l1 * a.st.s1 + l2 * a.st.s2), a.st.es,
-                       (const C*)a.st.mul, a.st.vn, a.st.ves, l0 * a.st.vls,
-                       a.tw_level ? l1 : l0,
-                       a.tw_N ? (const C*)a.tw_hi : nullptr, (const C*)a.tw_lo, a.tw_shift,
-                       a.tw_dir, (R)a.scale, ok};
+  if (u == 0) {
+    const int64_t l = ok ? line : 0;
+    const int64_t q0 = l % a.m0, t = l / a.m0;
+    const int64_t q1 = t % a.m1, q2 = t / a.m1;
+    lb[4 * g + 0] = q0;
+    lb[4 * g + 1] = q0 * a.ld.s0 + q1 * a.ld.s1 + q2 * a.ld.s2;
+    lb[4 * g + 2] = q0 * a.st.s0 + q1 * a.st.s1 + q2 * a.st.s2;
+    lb[4 * g + 3] = a.tw_level ? q1 : q0;
+  }
+  __syncthreads();
+  const int64_t l0 = lb[4 * g + 0], lt = lb[4 * g + 3];
   const C* tw = (const C*)a.prog.tw;
   const R* pcs = (const R*)a.prime_cs;
-  if constexpr (MID) {
-    fast_prog<R, -1, RL, T>(buf, in, SmemIO{}, tw, pcs, u);
-    const C* __restrict__ mid = (const C*)a.mid;
-    for (int k = u; k < L; k += T)
-      buf[padi(k)] = cmul<R>(buf[padi(k)], __ldg(mid + l0 * a.mid_ls + (int64_t)k * a.mid_es));
-    __syncthreads();
-    fast_prog<R, 1, RL, T>(buf, SmemIO{}, out, tw, pcs, u);
-  } else {
+  const C* ib = (const C*)a.in + lb[4 * g + 1];
+  C* ob = (C*)a.out + lb[4 * g + 2];
+  if constexpr (PLAIN && !MID) {
+    const C* tin = a.tw_on_load ? (const C*)a.tw_tab : nullptr;
+    const C* tout = a.tw_on_load ? nullptr : (const C*)a.tw_tab;
+    const PlainIn<R> in{ib, (int)a.ld.es, tin, (int)a.tw_es, (int)(lt * a.tw_ls), a.tw_dir};
+    const PlainOut<R> out{ob, (int)a.st.es, tout, (int)a.tw_es, (int)(lt * a.tw_ls), a.tw_dir,
+                          (R)a.scale, ok};
     if (a.dir1 < 0)
       fast_prog<R, -1, RL, T>(buf, in, out, tw, pcs, u);
     else
       fast_prog<R, 1, RL, T>(buf, in, out, tw, pcs, u);
+  } else {
+    const C* tin = a.tw_on_load ? (const C*)a.tw_tab : nullptr;
+    const C* tout = a.tw_on_load ? nullptr : (const C*)a.tw_tab;
+    const TileIn<R> in{ib, a.ld.es, (const C*)a.ld.mul, a.ld.vn, a.ld.ves, l0 * a.ld.vls, ok,
+                       tin, a.tw_es, lt * a.tw_ls, a.tw_dir};
+    const TileOut<R> out{ob, a.st.es, (const C*)a.st.mul, a.st.vn, a.st.ves, l0 * a.st.vls, lt,
+                         a.tw_N ? (const C*)a.tw_hi : nullptr, (const C*)a.tw_lo, a.tw_shift,
+                         a.tw_dir, (R)a.scale, ok, tout, a.tw_es, lt * a.tw_ls};
+    if constexpr (MID) {
+      fast_prog<R, -1, RL, T>(buf, in, SmemIO{}, tw, pcs, u);
+      const C* __restrict__ mid = (const C*)a.mid;
+      for (int k = u; k < L; k += T)
+        buf[padi(k)] = cmul<R>(buf[padi(k)], __ldg(mid + l0 * a.mid_ls + (int64_t)k * a.mid_es));
+      __syncthreads();
+      fast_prog<R, 1, RL, T>(buf, SmemIO{}, out, tw, pcs, u);
+    } else {
+      if (a.dir1 < 0)
+        fast_prog<R, -1, RL, T>(buf, in, out, tw, pcs, u);
+      else
+        fast_prog<R, 1, RL, T>(buf, in, out, tw, pcs, u);
+    }
   }
 }
 
@@ -323,15 +394,18 @@ template <typename R, class RL, int T> struct FastEntry {
     return e;
   }
   static cudaError_t launch_tile(const LineArgs& a, cudaStream_t s) {
-    static int set_plain[64] = {0}, set_mid[64] = {0};
-    const size_t smem = (size_t)a.G * LPAD * sizeof(cplx<R>);
+    static int set_plain[64] = {0}, set_mid[64] = {0}, set_full[64] = {0};
+    const size_t smem = (size_t)a.G * LPAD * sizeof(cplx<R>) + (size_t)a.G * 4 * sizeof(int64_t);
     const bool mid = a.mid != nullptr;
-    auto k = mid ? fast_tile_kernel<R, RL, T, true> : fast_tile_kernel<R, RL, T, false>;
+    auto k = mid ? fast_tile_kernel<R, RL, T, true, false>
+                 : (a.plain_io ? fast_tile_kernel<R, RL, T, false, true>
+                               : fast_tile_kernel<R, RL, T, false, false>);
+    int* set = mid ? set_mid : (a.plain_io ? set_plain : set_full);
     if (a.G * T > (T > 512 ? T : 512) || (mid && (a.dir1 > 0 || a.dir2 < 0))) {
       launch_failure(k, "tile launch shape", L, T, a.G, smem, cudaErrorInvalidValue);
       return cudaErrorInvalidValue;
     }
-    cudaError_t e = configure(k, smem, mid ? set_mid : set_plain);
+    cudaError_t e = configure(k, smem, set);
     if (e != cudaSuccess) {
       launch_failure(k, "tile smem attribute", L, T, a.G, smem, e);
       return e;

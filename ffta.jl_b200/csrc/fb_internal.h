@@ -54,6 +54,14 @@ struct LineArgs {
   int tw_dir, tw_shift, tw_level;
   const void* tw_hi;
   const void* tw_lo;
+  // or a full table (tw_tab != null, takes precedence): element i of line l
+  // is multiplied by tw_tab[i*tw_es + lt*tw_ls] (conjugated when tw_dir > 0)
+  const void* tw_tab;
+  int64_t tw_es, tw_ls;
+  int tw_on_load;       // 1: the twiddle multiplies element i of each line as
+                        // it is loaded (before the transform), not on store
+  int plain_io;         // 1: no presence window, no tables but tw_tab, and
+                        // |strides| * L < 2^31 (the tile kernel's lean I/O)
   double scale;         // applied on store when != 1
   int G, T;             // lines per block, threads per line
   int Lpad;             // smem elements per line
@@ -117,6 +125,9 @@ cudaError_t gen_stage_twiddles(int dtype, void* out, int R, int64_t Ns, cudaStre
 // out[q] = exp(sign * 2 pi i * ((q*step) mod N) / N) for q < count, sign = -1
 cudaError_t gen_roots(int dtype, void* out, int64_t N, int64_t step, int64_t count,
                       cudaStream_t s);
+// Full twiddle table: out[i*n_ln + l] = exp(-2 pi i (i*l mod N)/N).
+cudaError_t gen_tw_table(int dtype, void* out, int64_t N, int64_t n_el, int64_t n_ln,
+                         cudaStream_t s);
 // Bluestein chirp pieces for length N, pad M, direction dir (FFTA
 // src/algos.jl:344-367: b[n] = exp(i pi sgn n^2 / N), sgn = -dir):
 //   pre[n]  = conj(b[n])            n < N

@@ -158,6 +158,18 @@ __global__ void k_stage_tw(C* out, int R, int64_t Ns, int64_t count) {
   }
 }
 
+// out[i*n_ln + l] = exp(-2 pi i (i*l mod N) / N) for i < n_el, l < n_ln.
+template <typename C>
+__global__ void k_tw_table(C* out, int64_t N, int64_t n_el, int64_t n_ln) {
+  const int64_t count = n_el * n_ln;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < count;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = q / n_ln, l = q % n_ln;
+    const unsigned __int128 e = (unsigned __int128)i * (unsigned __int128)l;
+    out[q] = from_d2<C>(root_fp64((int64_t)(e % (unsigned __int128)N), N));
+  }
+}
+
 template <typename C>
 __global__ void k_roots(C* out, int64_t N, int64_t step, int64_t count) {
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < count;
@@ -248,6 +260,17 @@ cudaError_t gen_roots(int dtype, void* out, int64_t N, int64_t step, int64_t cou
     k_roots<float2><<<grid_for(count), 256, 0, s>>>((float2*)out, N, step, count);
   else
     k_roots<double2><<<grid_for(count), 256, 0, s>>>((double2*)out, N, step, count);
+  return cudaGetLastError();
+}
+
+cudaError_t gen_tw_table(int dtype, void* out, int64_t N, int64_t n_el, int64_t n_ln,
+                         cudaStream_t s) {
+  const int64_t count = n_el * n_ln;
+  if (count <= 0) return cudaSuccess;
+  if (dtype == 0)
+    k_tw_table<float2><<<grid_for(count), 256, 0, s>>>((float2*)out, N, n_el, n_ln);
+  else
+    k_tw_table<double2><<<grid_for(count), 256, 0, s>>>((double2*)out, N, n_el, n_ln);
   return cudaGetLastError();
 }
 

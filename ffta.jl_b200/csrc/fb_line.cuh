@@ -179,6 +179,10 @@ __device__ __forceinline__ void load_lines(const LineArgs& a, cplx<R>* sm, const
         if (vi < io.vn) {
           v = in[lb[g] + (int64_t)i * io.es];
           if (mul) v = cmul<R>(v, __ldg(mul + vi));
+          if (a.tw_on_load) {
+            const C w = __ldg((const C*)a.tw_tab + (int64_t)i * a.tw_es + lb[3 * G + g] * a.tw_ls);
+            v = (a.tw_dir < 0) ? cmul<R>(v, w) : cmulc<R>(v, w);
+          }
         }
       }
       sm[g * Lp + padi(i)] = v;
@@ -194,6 +198,10 @@ __device__ __forceinline__ void load_lines(const LineArgs& a, cplx<R>* sm, const
         if (vi < io.vn) {
           v = in[base + (int64_t)i * io.es];
           if (mul) v = cmul<R>(v, __ldg(mul + vi));
+          if (a.tw_on_load) {
+            const C w = __ldg((const C*)a.tw_tab + (int64_t)i * a.tw_es + lb[3 * G + g] * a.tw_ls);
+            v = (a.tw_dir < 0) ? cmul<R>(v, w) : cmulc<R>(v, w);
+          }
         }
       }
       sm[g * Lp + padi(i)] = v;
@@ -206,7 +214,10 @@ __device__ __forceinline__ cplx<R> finish(const LineArgs& a, cplx<R> v, int64_t 
                                           int64_t vi) {
   typedef cplx<R> C;
   if (a.st.mul) v = cmul<R>(v, __ldg((const C*)a.st.mul + vi));
-  if (a.tw_N) {
+  if (a.tw_tab && !a.tw_on_load) {
+    const C w = __ldg((const C*)a.tw_tab + (int64_t)i * a.tw_es + tfac * a.tw_ls);
+    v = (a.tw_dir < 0) ? cmul<R>(v, w) : cmulc<R>(v, w);
+  } else if (a.tw_N) {
     const int64_t e = tfac * (int64_t)i;
     const C hi = __ldg((const C*)a.tw_hi + (e >> a.tw_shift));
     const C lo = __ldg((const C*)a.tw_lo + (e & ((int64_t(1) << a.tw_shift) - 1)));

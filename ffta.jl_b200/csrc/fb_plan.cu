@@ -338,7 +338,7 @@ static void use_tile(const fb_plan_s* P, Pass& p, const std::vector<int>& radice
   const int es = elem_bytes(P->dtype);
   const int T = ff->T;
   const int thr_cap = std::max(1, std::max(512, T) / T);
-  const int smem_cap = (int)std::max<size_t>(1, (100 * 1024) / ((size_t)ff->lpad * es));
+  const int smem_cap = (int)std::max<size_t>(1, (100 * 1024) / ((size_t)ff->lpad * es + 32));
   const bool em = p.a.ld.mode == 1 || p.a.st.mode == 1;
   // strided tiles: as many neighbouring lines as the block allows (longer
   // contiguous runs per DRAM page); contiguous lines: 256-thread blocks
@@ -349,6 +349,15 @@ static void use_tile(const fb_plan_s* P, Pass& p, const std::vector<int>& radice
   p.staged = ff;
   p.a.T = T;
   p.a.G = std::max(1, G);
+  // lean I/O when nothing but strides, a full twiddle table and a scale is
+  // needed and every 32-bit offset fits
+  const int64_t L = p.a.prog.L;
+  const bool small = std::llabs(p.a.ld.es) * L < (int64_t(1) << 31) &&
+                     std::llabs(p.a.st.es) * L < (int64_t(1) << 31) &&
+                     (!p.a.tw_tab || (L * p.a.tw_es + p.a.tw_ls * (int64_t)p.a.nlines) < (int64_t(1) << 31));
+  p.a.plain_io = !p.a.mid && !p.a.ld.mul && !p.a.st.mul && p.a.ld.vn == INT64_MAX &&
+                 p.a.st.vn == INT64_MAX && !(p.a.tw_N && !p.a.tw_tab) && small &&
+                 p.a.ld.count == L && p.a.st.count == L;
   p.what += "[tile T=" + std::to_string(T) + " G=" + std::to_string(p.a.G) + "]";
 }
 
@@ -502,7 +511,24 @@ static void attach_blue(fb_plan_s* P, const LineX& x, LineArgs* a) {
 }
 
 // Two-level root tables for w_N^e, e < N: hi[e >> shift] * lo[e & mask].
-static void attach_twiddle(fb_plan_s* P, LineArgs* a, int64_t N, int dir) {
+// Four-step twiddle w_N^(e) for the elements i < n_el of the lines with
+// twiddle index lt < n_ln, e = i*lt.  Up to kFullTwiddle entries a full table
+// (one coalesced load per element: entry i*n_ln + lt) is made; beyond, the
+// two-level tables (hi[e >> shift] * lo[e & mask]).
+static const int64_t kFullTwiddle = int64_t(1) << 23;
+
+static void attach_twiddle(fb_plan_s* P, LineArgs* a, int64_t N, int dir, int64_t n_el,
+                           int64_t n_ln) {
+  a->tw_dir = dir;
+  if (n_el * n_ln <= kFullTwiddle) {
+    void* tab = alloc_table(P, (size_t)(n_el * n_ln) * elem_bytes(P->dtype));
+    cuda_check(gen_tw_table(P->dtype, tab, N, n_el, n_ln, 0), "twiddle table");
+    a->tw_tab = tab;
+    a->tw_es = n_ln;
+    a->tw_ls = 1;
+    a->tw_N = 0;
+    return;
+  }
   int shift = 0;
   while ((int64_t(1) << (2 * shift)) < N) ++shift;  // 2^shift >= sqrt(N)
   const int64_t lo_n = int64_t(1) << shift;
@@ -636,7 +662,7 @@ static Axis plan_direct_axis(fb_plan_s* P, int64_t n, LineX& x, int64_t is, int6
 // L2 residency.  With contiguous axes the batch is cut into chunks whose
 // scratch (N * chunk elements, at most kL2Chunk bytes) stays in L2 between
 // pass 1 and pass 2; the chunks run one after the other (host loop).
-static const size_t kL2Chunk = 32u << 20;
+static const size_t kL2Chunk = 64u << 20;
 
 static Axis plan_four_axis(fb_plan_s* P, int64_t N, int64_t N1, int64_t N2, LineX& x1, LineX& x2,
                            int64_t is, int64_t os, const std::vector<BDim>& bd, int src, int dst) {
@@ -714,8 +740,17 @@ static Axis plan_four_axis(fb_plan_s* P, int64_t N, int64_t N1, int64_t N2, Line
   }
   if (x1.kind == 1) attach_blue(P, x1, &p1.a);
   if (x2.kind == 1) attach_blue(P, x2, &p2.a);
-  attach_twiddle(P, &p1.a, N, P->dir);
-  p1.a.tw_level = tmode ? 1 : 0;
+  // the twiddle w_N^(n2 k1) multiplies the columns' outputs; with a full
+  // table it is applied as pass 2 loads them (element n2 of line k1), so its
+  // table loads issue with the data loads
+  if ((int64_t)N <= kFullTwiddle && x2.kind == 0) {
+    attach_twiddle(P, &p2.a, N, P->dir, N2, N1);
+    p2.a.tw_on_load = 1;
+    p2.a.tw_level = tmode ? 1 : 0;
+  } else {
+    attach_twiddle(P, &p1.a, N, P->dir, N1, N2);
+    p1.a.tw_level = tmode ? 1 : 0;
+  }
   p1.a.G = pick_G(P, x1.L, x1.T, p1.a.Lpad, true, p1.a.nlines);
   p2.a.G = pick_G(P, x2.L, x2.T, p2.a.Lpad, p2.a.ld.mode == 1 || p2.a.st.mode == 1,
                   p2.a.nlines);
@@ -773,7 +808,7 @@ static Axis plan_blue3_axis(fb_plan_s* P, int64_t N, int64_t is, int64_t os,
   p1.a.ld.ves = M2;
   p1.a.ld.vls = 1;
   p1.a.st = io_plain(1, M, B0 * M, M2, (int)M1);
-  attach_twiddle(P, &p1.a, M, FB_FORWARD);
+  if (M > kFullTwiddle) attach_twiddle(P, &p1.a, M, FB_FORWARD, M1, M2);
   p1.a.ld.mode = is == 1 ? 1 : 0;
   p1.a.st.mode = 1;
   p1.a.G = pick_G(P, x1.L, x1.T, p1.a.Lpad, true, p1.a.nlines);
@@ -793,7 +828,12 @@ static Axis plan_blue3_axis(fb_plan_s* P, int64_t N, int64_t is, int64_t os,
   p2.a.mid_es = M1;
   p2.a.dir1 = FB_FORWARD;
   p2.a.dir2 = FB_BACKWARD;
-  attach_twiddle(P, &p2.a, M, FB_BACKWARD);
+  if (M <= kFullTwiddle) {
+    // pass 1's twiddle w_M^(n2 k1), applied as pass 2 loads (element n2 of line k1)
+    attach_twiddle(P, &p2.a, M, FB_FORWARD, M2, M1);
+    p2.a.tw_on_load = 1;
+  }
+  if (M > kFullTwiddle) attach_twiddle(P, &p2.a, M, FB_BACKWARD, M2, M1);
   p2.a.ld.mode = 0;
   p2.a.st.mode = 1;
   p2.a.G = pick_G(P, x2.L, x2.T, p2.a.Lpad, true, p2.a.nlines);
@@ -814,6 +854,12 @@ static Axis plan_blue3_axis(fb_plan_s* P, int64_t N, int64_t is, int64_t os,
   p3.a.st.vls = 1;
   p3.a.ld.mode = 0;
   p3.a.st.mode = os == 1 ? 1 : 0;
+  if (M <= kFullTwiddle) {
+    // the conjugate twiddle of pass 2's outputs, applied as pass 3 loads them
+    // (element k1 of line m2)
+    attach_twiddle(P, &p3.a, M, FB_BACKWARD, M1, M2);
+    p3.a.tw_on_load = 1;
+  }
   p3.a.G = pick_G(P, x1.L, x1.T, p3.a.Lpad, p3.a.st.mode == 1, p3.a.nlines);
   std::ostringstream w;
   w << "BLUE3(N=" << N << " M=" << M1 << "x" << M2 << ")";
