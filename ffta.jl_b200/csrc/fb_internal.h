@@ -140,4 +140,13 @@ cudaError_t convert_c64(int dtype, void* dst, const void* src_c64, int64_t n, do
                         cudaStream_t s);
 cudaError_t gen_prime_tables(void* f32tab, void* f64tab, cudaStream_t s);
 
+// Real-transform helpers on contiguous column-major arrays (dtype 0: float /
+// ComplexF32, 1: double / ComplexF64).
+cudaError_t real_to_complex(int dtype, const void* in, void* out, int64_t count, cudaStream_t s);
+cudaError_t complex_to_real(int dtype, const void* in, void* out, int64_t count, cudaStream_t s);
+cudaError_t extract_half(int dtype, const void* in, void* out, int64_t pre, int64_t n, int64_t h,
+                         int64_t post, cudaStream_t s);
+cudaError_t herm_extend(int dtype, const void* x, void* z, int rank, const int64_t* dims, int r0,
+                        int64_t h, uint32_t region, cudaStream_t s);
+
 }  // namespace fb

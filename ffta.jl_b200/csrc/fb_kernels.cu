@@ -20,6 +20,8 @@
 // twiddle comes from a table computed in FP64 and rounded once.
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 #include "fb_device.cuh"
 #include "fb_internal.h"
 
@@ -292,6 +294,128 @@ cudaError_t convert_c64(int dtype, void* dst, const void* src_c64, int64_t n, do
   else
     k_convert<double2><<<grid_for(n), 256, 0, s>>>((double2*)dst, (const double2*)src_c64, n,
                                                    scale);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------ real transforms
+// Column-major arrays; `dims` (rank <= 8) are the full (complex) dims.
+struct RealGeom {
+  int rank, r0;
+  int64_t dims[8];
+  int64_t h;        // n/2 + 1 along r0
+  uint32_t region;  // bit d: dim d is transformed
+};
+
+template <typename R>
+__global__ void k_real_to_complex(const R* __restrict__ in, cplx<R>* __restrict__ out,
+                                  int64_t count) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = Sc<R>::mk(in[i], R(0));
+}
+
+template <typename R>
+__global__ void k_complex_to_real(const cplx<R>* __restrict__ in, R* __restrict__ out,
+                                  int64_t count) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = in[i].x;
+}
+
+// out (dims with r0 cut to h) <- in (full dims): the first h entries along r0
+template <typename R>
+__global__ void k_extract_half(const cplx<R>* __restrict__ in, cplx<R>* __restrict__ out,
+                               int64_t pre, int64_t n, int64_t h, int64_t post) {
+  const int64_t count = pre * h * post;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < count;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t a = q % pre, t = q / pre, k = t % h, b = t / h;
+    out[q] = in[a + pre * (k + n * b)];
+  }
+}
+
+// z (full dims) <- Hermitian extension of x (r0 cut to h): entries with index
+// k < h along r0 are copied; the others are conj(x at the mirrored index
+// (-k mod n) in every transformed dim), the symmetry of a real signal's
+// spectrum.
+template <typename R>
+__global__ void k_herm_extend(const cplx<R>* __restrict__ x, cplx<R>* __restrict__ z,
+                              RealGeom g) {
+  int64_t total = 1;
+  for (int d = 0; d < g.rank; ++d) total *= g.dims[d];
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    int64_t idx[8];
+    int64_t t = q;
+    for (int d = 0; d < g.rank; ++d) {
+      idx[d] = t % g.dims[d];
+      t /= g.dims[d];
+    }
+    const bool mirror = idx[g.r0] >= g.h;
+    if (mirror)
+      for (int d = 0; d < g.rank; ++d)
+        if ((g.region >> d) & 1) idx[d] = idx[d] ? g.dims[d] - idx[d] : 0;
+    int64_t src = 0, stride = 1;
+    for (int d = 0; d < g.rank; ++d) {
+      src += idx[d] * stride;
+      stride *= d == g.r0 ? g.h : g.dims[d];
+    }
+    const cplx<R> v = x[src];
+    z[q] = mirror ? Sc<R>::mk(v.x, -v.y) : v;
+  }
+}
+
+cudaError_t real_to_complex(int dtype, const void* in, void* out, int64_t count, cudaStream_t s) {
+  if (count <= 0) return cudaSuccess;
+  if (dtype == 0)
+    k_real_to_complex<float><<<grid_for(count), 256, 0, s>>>((const float*)in, (float2*)out, count);
+  else
+    k_real_to_complex<double><<<grid_for(count), 256, 0, s>>>((const double*)in, (double2*)out,
+                                                               count);
+  return cudaGetLastError();
+}
+
+cudaError_t complex_to_real(int dtype, const void* in, void* out, int64_t count, cudaStream_t s) {
+  if (count <= 0) return cudaSuccess;
+  if (dtype == 0)
+    k_complex_to_real<float><<<grid_for(count), 256, 0, s>>>((const float2*)in, (float*)out, count);
+  else
+    k_complex_to_real<double><<<grid_for(count), 256, 0, s>>>((const double2*)in, (double*)out,
+                                                              count);
+  return cudaGetLastError();
+}
+
+cudaError_t extract_half(int dtype, const void* in, void* out, int64_t pre, int64_t n, int64_t h,
+                         int64_t post, cudaStream_t s) {
+  const int64_t count = pre * h * post;
+  if (count <= 0) return cudaSuccess;
+  if (dtype == 0)
+    k_extract_half<float><<<grid_for(count), 256, 0, s>>>((const float2*)in, (float2*)out, pre, n,
+                                                          h, post);
+  else
+    k_extract_half<double><<<grid_for(count), 256, 0, s>>>((const double2*)in, (double2*)out, pre,
+                                                           n, h, post);
+  return cudaGetLastError();
+}
+
+cudaError_t herm_extend(int dtype, const void* x, void* z, int rank, const int64_t* dims, int r0,
+                        int64_t h, uint32_t region, cudaStream_t s) {
+  RealGeom g;
+  memset(&g, 0, sizeof(g));
+  g.rank = rank;
+  g.r0 = r0;
+  g.h = h;
+  g.region = region;
+  int64_t total = 1;
+  for (int d = 0; d < rank; ++d) {
+    g.dims[d] = dims[d];
+    total *= dims[d];
+  }
+  if (total <= 0) return cudaSuccess;
+  if (dtype == 0)
+    k_herm_extend<float><<<grid_for(total), 256, 0, s>>>((const float2*)x, (float2*)z, g);
+  else
+    k_herm_extend<double><<<grid_for(total), 256, 0, s>>>((const double2*)x, (double2*)z, g);
   return cudaGetLastError();
 }
 

@@ -305,6 +305,14 @@ struct fb_plan_s {
   std::unique_ptr<fb::DevBuf> hin, hout;
   // grouped execution: device copy of the request descriptors
   std::unique_ptr<fb::DevBuf> desc;
+  // real transforms (rfft: 1, brfft: 2): a complex plan over the full dims run
+  // in place on zbuf, between a conversion in and an extraction out
+  int real_kind = 0;
+  std::unique_ptr<fb_plan_s> cplan;
+  std::unique_ptr<fb::DevBuf> zbuf;
+  int r0 = 0;
+  int64_t rh = 0;
+  uint32_t region_mask = 0;
   // pipelined host execution: plans for one chunk and the last one, device
   // slots, streams and events
   std::unique_ptr<fb_plan_s> chunk_plan, tail_plan;
@@ -1006,7 +1014,13 @@ static fb_plan_s* create_plan(int dtype, int dir, int rank, const int64_t* dims,
   return P.release();
 }
 
+static void execute_real(fb_plan_s* P, const void* in, void* out, cudaStream_t s);
+
 static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s) {
+  if (P->real_kind) {
+    execute_real(P, in, out, s);
+    return;
+  }
   int dev = 0;
   cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
   if (dev != P->device) fail(FB_ERR_ARGUMENT, "plan was created on another device");
@@ -1201,14 +1215,15 @@ int fb_execute_host(fb_plan plan, const void* in, void* out, void* stream) {
   return guard([&] {
     if (!plan) fail(FB_ERR_ARGUMENT, "null plan");
     if (plan->in_span == 0) return;
-    if (host_pipeline(plan, in, out)) return;
+    if (!plan->real_kind && host_pipeline(plan, in, out)) return;
     const int es = elem_bytes(plan->dtype);
-    const size_t ib = (size_t)plan->in_span * es, ob = (size_t)plan->out_span * es;
+    const int ies = plan->real_kind == 1 ? es / 2 : es, oes = plan->real_kind == 2 ? es / 2 : es;
+    const size_t ib = (size_t)plan->in_span * ies, ob = (size_t)plan->out_span * oes;
     if (!plan->hin || plan->hin->bytes < ib) plan->hin.reset(new DevBuf(ib));
     if (!plan->hout || plan->hout->bytes < ob) plan->hout.reset(new DevBuf(ob));
     cudaStream_t s = (cudaStream_t)stream;
     cuda_check(cudaMemcpyAsync(plan->hin->p, in, ib, cudaMemcpyHostToDevice, s), "copy in");
-    if (ob > ib || plan->out_span != plan->in_span) {
+    if (!plan->real_kind && (ob > ib || plan->out_span != plan->in_span)) {
       // outputs that no pass writes keep the host's values
       cuda_check(cudaMemcpyAsync(plan->hout->p, out, ob, cudaMemcpyHostToDevice, s), "copy out init");
     }
@@ -1324,6 +1339,90 @@ const char* fb_last_error(void) { return g_last_error.c_str(); }
 const char* fb_version(void) { return FB_VERSION; }
 
 }  // extern "C"
+
+// ============================================================ real transforms
+// rfft (src/plan.jl:102-125, 390-454, 506-542): the real input becomes the
+// complex array x + 0i, the complex plan transforms it, and the first n/2+1
+// entries along the first region dim are kept.  brfft (src/plan.jl:127-150,
+// 456-504, 544-583): the n/2+1 stored entries are extended to the full
+// Hermitian spectrum (mirrored in every region dim), the backward complex
+// plan transforms it, and the real part is kept.  FFTA computes even lengths
+// through a half-length complex transform and a split; the results agree to
+// rounding.
+namespace fb {
+
+static fb_plan_s* create_real_plan(int dtype, int dir, int rank, const int64_t* dims,
+                                   const std::vector<int>& region, int64_t cutoff, uint32_t flags) {
+  if (region.empty()) fail(FB_ERR_ARGUMENT, "a real transform needs at least one region dim");
+  std::vector<int64_t> st(rank);
+  int64_t total = 1;
+  for (int d = 0; d < rank; ++d) {
+    if (dims[d] < 0) fail(FB_ERR_DIMENSION_MISMATCH, "negative dimension");
+    st[d] = total;
+    total *= dims[d];
+  }
+  std::unique_ptr<fb_plan_s> C(create_plan(dtype, dir, rank, dims, st.data(), st.data(), region,
+                                           cutoff, flags));
+  std::unique_ptr<fb_plan_s> P(new fb_plan_s());
+  P->dtype = dtype;
+  P->dir = dir;
+  P->cutoff = cutoff;
+  P->flags = flags;
+  P->rank = rank;
+  P->dims.assign(dims, dims + rank);
+  P->istrides = st;
+  P->ostrides = st;
+  P->region = region;
+  P->device = C->device;
+  P->real_kind = dir == FB_FORWARD ? 1 : 2;
+  P->r0 = region[0];
+  P->rh = dims[P->r0] / 2 + 1;
+  for (int r : region) P->region_mask |= 1u << r;
+  const int64_t half = total / std::max<int64_t>(1, dims[P->r0]) * P->rh;
+  // spans counted in elements of each side's own type (real or complex)
+  P->in_span = P->real_kind == 1 ? total : half;
+  P->out_span = P->real_kind == 1 ? half : total;
+  if (total > 0) P->zbuf.reset(new DevBuf((size_t)total * elem_bytes(dtype)));
+  P->cplan = std::move(C);
+  return P.release();
+}
+
+static void execute_real(fb_plan_s* P, const void* in, void* out, cudaStream_t s) {
+  int64_t total = 1, pre = 1, post = 1;
+  for (int d = 0; d < P->rank; ++d) {
+    total *= P->dims[d];
+    if (d < P->r0) pre *= P->dims[d];
+    if (d > P->r0) post *= P->dims[d];
+  }
+  if (total == 0) return;
+  P->cplan->scale = P->scale;
+  void* z = P->zbuf->p;
+  if (P->real_kind == 1) {
+    cuda_check(real_to_complex(P->dtype, in, z, total, s), "real to complex");
+    execute_plan(P->cplan.get(), z, z, s);
+    cuda_check(extract_half(P->dtype, z, out, pre, P->dims[P->r0], P->rh, post, s), "extract");
+  } else {
+    cuda_check(herm_extend(P->dtype, in, z, P->rank, P->dims.data(), P->r0, P->rh,
+                           P->region_mask, s), "hermitian extension");
+    execute_plan(P->cplan.get(), z, z, s);
+    cuda_check(complex_to_real(P->dtype, z, out, total, s), "complex to real");
+  }
+}
+
+}  // namespace fb
+
+extern "C" int fb_plan_create_real(fb_plan* plan, int dtype, int dir, int rank,
+                                   const int64_t* dims, int nregion, const int32_t* region,
+                                   int64_t bluestein_cutoff, uint32_t flags) {
+  return guard([&] {
+    if (!plan) fail(FB_ERR_ARGUMENT, "plan pointer is null");
+    *plan = nullptr;
+    if (rank < 1 || rank > 8 || !dims) fail(FB_ERR_ARGUMENT, "bad array description");
+    std::vector<int> reg;
+    for (int i = 0; i < nregion; ++i) reg.push_back(region[i] - 1);
+    *plan = create_real_plan(dtype, dir, rank, dims, reg, bluestein_cutoff, flags);
+  });
+}
 
 // ===================================================================== server
 // Continuous batching over work-descriptor launches.  Requests (n, type,

@@ -31,7 +31,8 @@ from ._lib import lib
 __all__ = [
     "FFT_FORWARD", "FFT_BACKWARD", "DEFAULT_BLUESTEIN_CUTOFF", "DimensionMismatch",
     "ArgumentError", "DomainError", "CudaError", "UnsupportedError", "FFTAPlan_cx", "plan_fft",
-    "plan_bfft", "plan_ifft", "fft", "bfft", "ifft", "mul_", "size", "version",
+    "plan_bfft", "plan_ifft", "fft", "bfft", "ifft", "mul_", "size", "version", "FFTAPlan_re",
+    "plan_rfft", "plan_brfft", "plan_irfft", "rfft", "brfft", "irfft",
 ]
 
 FFT_FORWARD = -1  # src/callgraph.jl:1
@@ -431,3 +432,216 @@ def bfft(x, region=None, **kw):
 def ifft(x, region=None, **kw):
     """AbstractFFTs ifft: bfft scaled by 1/prod(sizes along region)."""
     return _apply(plan_ifft, x, region, **kw)
+
+
+# -------------------------------------------------------- real transforms
+def _real_kind(x) -> str:
+    """'f32' / 'f64' for real inputs, 'c64' / 'c128' for complex, else raise."""
+    if _is_torch(x):
+        torch = _torch()
+        k = {torch.float32: "f32", torch.float64: "f64", torch.complex64: "c64",
+             torch.complex128: "c128"}.get(x.dtype)
+    else:
+        k = {np.dtype(np.float32): "f32", np.dtype(np.float64): "f64",
+             np.dtype(np.complex64): "c64", np.dtype(np.complex128): "c128"}.get(
+                 np.asarray(x).dtype)
+    if k is None:
+        raise ArgumentError(f"element type {x.dtype} is not supported: only Float32/Float64 "
+                            "(and their complex types) run on the GPU, and there is no CPU "
+                            "fallback")
+    return k
+
+
+def _col_major(x):
+    """x as contiguous column-major memory (Julia layout) plus its dims."""
+    if _is_torch(x):
+        perm = tuple(range(x.ndim - 1, -1, -1))
+        return x.permute(perm).contiguous(), tuple(int(s) for s in x.shape)
+    return np.asfortranarray(x), tuple(int(s) for s in x.shape)
+
+
+class FFTAPlan_re:
+    """A real transform plan (FFTA's FFTAPlan_re, src/plan.jl:22-34).
+
+    dir FFT_FORWARD: rfft (real input, n/2+1 outputs along the first region
+    dim); FFT_BACKWARD: brfft of length `flen` (complex input, real output).
+    """
+
+    def __init__(self, sizes, region, direction, prec, flen, cutoff, scale=1.0):
+        self._sizes = tuple(sizes)
+        self.region = region
+        self.dir = direction
+        self._prec = prec  # "f32" / "f64"
+        self.flen = int(flen)
+        self.BLUESTEIN_CUTOFF = cutoff
+        self.scale = scale
+        self._cplans = {}
+
+    def size(self, i=None):
+        """Base.size (src/plan.jl:36-47): the real length first."""
+        sz = (self.flen,) + self._sizes[1:]
+        if i is None:
+            return sz
+        i = int(i)
+        if i < 1:
+            raise DomainError(f"{i}: No non-positive dimensions")
+        return sz[i - 1] if i <= len(sz) else 1
+
+    @property
+    def ndims(self):
+        return len(self._sizes)
+
+    def __del__(self):
+        try:
+            for h in self._cplans.values():
+                lib.fb_plan_destroy(h)
+        except Exception:
+            pass
+
+    def _regions(self):
+        r = self.region
+        return [r] if isinstance(r, int) else list(r)
+
+    def _handle(self, dims):
+        h = self._cplans.get(dims)
+        if h is None:
+            reg = self._regions()
+            cd = (ctypes.c_int64 * len(dims))(*dims)
+            cr = (ctypes.c_int32 * len(reg))(*reg)
+            hh = ctypes.c_void_p()
+            dt = _lib.FB_C32 if self._prec == "f32" else _lib.FB_C64
+            _check(lib.fb_plan_create_real(ctypes.byref(hh), dt, self.dir, len(dims), cd,
+                                           len(reg), cr, int(self.BLUESTEIN_CUTOFF), 0))
+            if self.scale != 1.0:
+                _check(lib.fb_plan_set_scale(hh, float(self.scale)))
+            self._cplans[dims] = hh
+            h = hh
+        return h
+
+    def __mul__(self, x):
+        kind = _real_kind(x)
+        vec = x.ndim == 1
+        what = "vectors" if vec else "arrays"
+        reg = self._regions()
+        if kind in ("f32", "f64"):
+            # src/plan.jl:390-393, 508-511, 532-535
+            if self.dir != FFT_FORWARD:
+                raise ArgumentError(f"only FFT_FORWARD supported for real {what}")
+            if kind != self._prec:
+                raise ArgumentError("plan is for another precision")
+            dims = tuple(int(s) for s in x.shape)
+            if reg[-1] > x.ndim or reg[0] < 1:
+                raise DimensionMismatch("Plan region is outside array dimensions.")
+            got = tuple(dims[r - 1] for r in reg)
+            if got != (self.flen,) + self._sizes[1:]:
+                raise DimensionMismatch(
+                    f"plan has size {self.size()}, but input array has size {got}")
+            out_dims = list(dims)
+            out_dims[reg[0] - 1] = self.flen // 2 + 1
+            return self._run(x, dims, tuple(out_dims), complex_out=True)
+        # complex input: brfft (src/plan.jl:457-460, 517-520, 545-548)
+        if self.dir != FFT_BACKWARD:
+            raise ArgumentError(f"only FFT_BACKWARD supported for complex {what}")
+        if {"c64": "f32", "c128": "f64"}[kind] != self._prec:
+            raise ArgumentError("plan is for another precision")
+        xs = tuple(int(s) for s in x.shape)
+        if reg[-1] > x.ndim or reg[0] < 1:
+            raise DimensionMismatch("Plan region is outside array dimensions.")
+        rlen = self.flen // 2 + 1
+        if xs[reg[0] - 1] != rlen:
+            raise DimensionMismatch(
+                f"real {len(reg)}D plan has size {self.flen}. Dimension of input array along "
+                f"region {reg[0]} should have size {rlen}, but has size {xs[reg[0] - 1]}")
+        if tuple(xs[r - 1] for r in reg[1:]) != self._sizes[1:]:
+            raise DimensionMismatch(f"real {len(reg)}D plan has size {self.size()}")
+        dims = list(xs)
+        dims[reg[0] - 1] = self.flen
+        return self._run(x, tuple(dims), tuple(dims), complex_out=False)
+
+    def _run(self, x, dims, out_dims, complex_out):
+        """Execute on `x`; `dims` are the real-array dims the plan is made for."""
+        if any(d == 0 for d in dims):
+            raise DimensionMismatch("Array length must be strictly positive")
+        h = self._handle(dims)
+        xc, _ = _col_major(x)
+        if _is_torch(x):
+            torch = _torch()
+            if complex_out:
+                odt = torch.complex64 if self._prec == "f32" else torch.complex128
+            else:
+                odt = torch.float32 if self._prec == "f32" else torch.float64
+            y = torch.empty(tuple(reversed(out_dims)), dtype=odt, device=x.device)
+            stream = torch.cuda.current_stream(x.device).cuda_stream
+            with torch.cuda.device(x.device):
+                _check(lib.fb_execute(h, ctypes.c_void_p(xc.data_ptr()),
+                                      ctypes.c_void_p(y.data_ptr()), ctypes.c_void_p(stream)))
+            return y.permute(tuple(range(y.ndim - 1, -1, -1)))
+        if complex_out:
+            odt = np.complex64 if self._prec == "f32" else np.complex128
+        else:
+            odt = np.float32 if self._prec == "f32" else np.float64
+        y = np.empty(out_dims, dtype=odt, order="F")
+        _check(lib.fb_execute_host(h, ctypes.c_void_p(xc.ctypes.data),
+                                   ctypes.c_void_p(y.ctypes.data), None))
+        return y
+
+
+def _real_region(x, region):
+    stored, srt = _normalize_region(region, x.ndim)
+    if len(srt) > 2:
+        raise ArgumentError("only supports 1D and 2D FFTs")
+    return stored, srt
+
+
+def plan_rfft(x, region=None, *, BLUESTEIN_CUTOFF=DEFAULT_BLUESTEIN_CUTOFF, **_kwargs):
+    """AbstractFFTs.plan_rfft (FFTA src/plan.jl:102-125)."""
+    if not _is_torch(x):
+        x = np.asarray(x)
+    kind = _real_kind(x)
+    if kind not in ("f32", "f64"):
+        raise ArgumentError("plan_rfft needs a real array")
+    stored, srt = _real_region(x, region)
+    shape = tuple(int(s) for s in x.shape)
+    sizes = tuple(shape[r - 1] if 1 <= r <= x.ndim else 1 for r in srt)
+    if any(v <= 0 for v in sizes):
+        raise DimensionMismatch("Array length must be strictly positive")
+    return FFTAPlan_re(sizes, stored, FFT_FORWARD, kind, sizes[0], int(BLUESTEIN_CUTOFF))
+
+
+def plan_brfft(x, len_, region=None, *, BLUESTEIN_CUTOFF=DEFAULT_BLUESTEIN_CUTOFF, _scale=False,
+               **_kwargs):
+    """AbstractFFTs.plan_brfft(x, len, region) (FFTA src/plan.jl:127-150)."""
+    if not _is_torch(x):
+        x = np.asarray(x)
+    kind = _real_kind(x)
+    prec = {"c64": "f32", "c128": "f64", "f32": "f32", "f64": "f64"}[kind]
+    stored, srt = _real_region(x, region)
+    shape = tuple(int(s) for s in x.shape)
+    sizes = (int(len_),) + tuple(shape[r - 1] if 1 <= r <= x.ndim else 1 for r in srt[1:])
+    if any(v <= 0 for v in sizes):
+        raise DimensionMismatch("Array length must be strictly positive")
+    scale = 1.0 / float(np.prod(sizes)) if _scale else 1.0
+    return FFTAPlan_re(sizes, stored, FFT_BACKWARD, prec, int(len_), int(BLUESTEIN_CUTOFF), scale)
+
+
+def plan_irfft(x, len_, region=None, **kw):
+    """AbstractFFTs.plan_irfft: plan_brfft scaled by 1/prod(sizes)."""
+    return plan_brfft(x, len_, region, _scale=True, **kw)
+
+
+def rfft(x, region=None, **kw):
+    if not _is_torch(x):
+        x = np.asarray(x)
+    return plan_rfft(x, region, **kw) * x
+
+
+def brfft(x, len_, region=None, **kw):
+    if not _is_torch(x):
+        x = np.asarray(x)
+    return plan_brfft(x, len_, region, **kw) * x
+
+
+def irfft(x, len_, region=None, **kw):
+    if not _is_torch(x):
+        x = np.asarray(x)
+    return plan_irfft(x, len_, region, **kw) * x

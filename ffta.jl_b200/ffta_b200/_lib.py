@@ -35,6 +35,9 @@ SIGNATURES = {
     "fb_plan_create_nd": ([_plan_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _i64p, _i64p, _i64p,
                            ctypes.c_int, ctypes.POINTER(ctypes.c_int32), _i64, ctypes.c_uint32],
                           ctypes.c_int),
+    "fb_plan_create_real": ([_plan_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _i64p,
+                             ctypes.c_int, ctypes.POINTER(ctypes.c_int32), _i64, ctypes.c_uint32],
+                            ctypes.c_int),
     "fb_plan_set_scale": ([_vp, ctypes.c_double], ctypes.c_int),
     "fb_execute": ([_vp, _vp, _vp, _vp], ctypes.c_int),
     "fb_execute_host": ([_vp, _vp, _vp, _vp], ctypes.c_int),

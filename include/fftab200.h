@@ -87,6 +87,20 @@ int fb_plan_create_nd(fb_plan* plan, int dtype, int dir, int rank, const int64_t
                       const int64_t* istrides, const int64_t* ostrides, int nregion,
                       const int32_t* region, int64_t bluestein_cutoff, uint32_t flags);
 
+/* Real transforms over a contiguous column-major array.  dir FB_FORWARD is
+ * rfft: real input with dims[], complex output whose first region dim holds
+ * dims[r]/2+1 entries (AbstractFFTs.plan_rfft, FFTA src/plan.jl:102-125 and
+ * the real executors :390-454, :506-542).  dir FB_BACKWARD is brfft: complex
+ * input with dims[r]/2+1 entries along the first region dim, real output
+ * with dims[] (plan_brfft, src/plan.jl:127-150, :456-504, :544-583); dims[r]
+ * is brfft's `len`.  dtype FB_C32 pairs Float32 with ComplexF32, FB_C64
+ * Float64 with ComplexF64.  FFTA allows one or two region dims ("only
+ * supports 1D and 2D FFTs"); this entry point takes any number.  irfft is
+ * brfft scaled by 1/prod(len) (fb_plan_set_scale). */
+int fb_plan_create_real(fb_plan* plan, int dtype, int dir, int rank, const int64_t* dims,
+                        int nregion, const int32_t* region, int64_t bluestein_cutoff,
+                        uint32_t flags);
+
 /* Multiply every output by `scale` (fused into the last kernel).  ifft is
  * bfft scaled by 1/prod(n) (AbstractFFTs ScaledPlan). */
 int fb_plan_set_scale(fb_plan plan, double scale);
