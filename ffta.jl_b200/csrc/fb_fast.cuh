@@ -175,6 +175,16 @@ template <typename R> struct PlainOut {
   }
 };
 
+// Element i of a line held flat (unpadded) in shared memory: the landing
+// buffer of a bulk copy (fast_stream_kernel).  Stage 0 then overwrites the
+// same buffer in the padded layout, after a barrier.
+template <typename R> struct FlatIn {
+  const cplx<R>* p;
+  __device__ __forceinline__ cplx<R> operator()(int i) const { return p[i]; }
+};
+template <class In> struct InIsSmem : std::false_type {};
+template <typename R> struct InIsSmem<FlatIn<R>> : std::true_type {};
+
 // ------------------------------------------------------------- stages
 // Stage S of program RL on one line held at `buf` (padded layout).  Thread u
 // of T owns butterflies j = u + q*T.  The first stage takes its inputs from
@@ -206,16 +216,16 @@ __device__ __forceinline__ void fast_stage(cplx<R>* buf, const In& in, const Out
   }
   // in place: all reads of the line finish before any write, unless one side
   // is global memory
-  if constexpr (!GIN && !GOUT) __syncthreads();
+  if constexpr ((!GIN || InIsSmem<In>::value) && !GOUT) __syncthreads();
 #pragma unroll
   for (int q = 0; q < UM; ++q) {
     const int j = u + q * T;
     if (nb % T == 0 || j < nb) {
       const int k = (Ns == 1) ? 0 : j % Ns;
       if constexpr (Ns > 1) {
-        const cplx<R>* w = tw + tw_offset<RL, S>() + k * (RAD - 1) - 1;
+        const cplx<R>* w = tw + tw_offset<RL, S>() + k;  // entry (r-1)*Ns + k
 #pragma unroll
-        for (int r = 1; r < RAD; ++r) v[q][r] = ctw<R, DIR>(v[q][r], __ldg(w + r));
+        for (int r = 1; r < RAD; ++r) v[q][r] = ctw<R, DIR>(v[q][r], __ldg(w + (r - 1) * Ns));
       }
       butterfly<R, RAD, DIR>(v[q], pcs);
       const int base = (j - k) * RAD + k;
@@ -276,6 +286,136 @@ __global__ void __launch_bounds__(DirectBounds<R, T>::threads, DirectBounds<R, T
   const DirectIn<R> in{gin, ok};
   const DirectOut<R> out{gout, ok, (R)a.scale};
   fast_prog<R, DIR, RL, T>(buf, in, out, (const C*)a.tw, (const R*)a.prime_cs, threadIdx.x);
+}
+
+// ------------------------------------------------------ stream kernel
+// Persistent variant of the direct kernel for contiguous lines whose bytes
+// start on 16-byte boundaries.  Block b transforms lines b, b + gridDim.x, ...
+// One thread keeps NBUF-1 lines ahead in flight as bulk asynchronous copies
+// (cp.async.bulk global -> shared, completion counted in bytes on one
+// mbarrier per buffer), so HBM reads continue while the block computes.
+// Stage 0 reads the flat copy, the later stages the padded layout in the same
+// buffer, and the last stage stores to HBM from registers.  The arithmetic is
+// that of the other kernels.  Every wait is bounded: after about a second the
+// block sets kErrWaitTimeout, waits (again bounded) for its copies in flight
+// and returns.
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(b)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_addr(b)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Wait for phase `parity` of *b for at most ~1 s; false if it gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
+  if (mbar_test(b, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 0; it < (1u << 30); ++it) {
+    if (mbar_test(b, parity)) return true;
+    if ((it & 63) == 63 && global_ns() - t0 > 1000000000ull) return false;
+  }
+  return false;
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* b) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(b))
+      : "memory");
+}
+
+template <typename R, class RL> struct StreamShape {
+  static constexpr int L = prog_len<RL>();
+  static constexpr uint32_t bytes = (uint32_t)(L * sizeof(cplx<R>));
+  // buffer stride: the padded line, rounded to 128 bytes
+  static constexpr size_t stride = ((size_t)lpad_of(L) * sizeof(cplx<R>) + 127) / 128 * 128;
+  static constexpr int nbuf = 2;
+  static constexpr size_t smem = 128 + nbuf * stride;
+  // lines of at least 4 KB, whole 16-byte units, two blocks per SM
+  static constexpr bool ok = bytes >= 4096 && bytes % 16 == 0 && smem <= 110 * 1024;
+};
+// Resident blocks per SM asked of the compiler: as many as shared memory
+// allows (227 KB, 1 KB reserved per block), at most 2048 threads, and never
+// below 64 registers per thread.
+template <typename R, class RL, int T> struct StreamBounds {
+  static constexpr int by_smem = (int)(232448 / (StreamShape<R, RL>::smem + 1024));
+  static constexpr int by_thr = 2048 / T;
+  static constexpr int by_reg = 65536 / (T * 64);
+  static constexpr int m0 = by_smem < by_thr ? by_smem : by_thr;
+  static constexpr int m1 = m0 < by_reg ? m0 : by_reg;
+  static constexpr int min_blocks = m1 < 1 ? 1 : m1;
+};
+
+template <typename R, int DIR, class RL, int T>
+__global__ void __launch_bounds__(T, StreamBounds<R, RL, T>::min_blocks)
+    fast_stream_kernel(const FastArgs a) {
+  typedef cplx<R> C;
+  typedef StreamShape<R, RL> SS;
+  constexpr int NBUF = SS::nbuf;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  uint64_t* bar = (uint64_t*)smraw;
+  auto buffer = [&](int b) { return (C*)(smraw + 128 + (size_t)b * SS::stride); };
+  const int u = threadIdx.x;
+  const int64_t first = blockIdx.x, step = gridDim.x;
+  const int64_t nmine = first < a.nlines ? (a.nlines - 1 - first) / step + 1 : 0;
+  const C* gin = (const C*)a.in;
+  C* gout = (C*)a.out;
+  if (u == 0) {
+    for (int b = 0; b < NBUF; ++b) mbar_init(bar + b, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int b = 0; b < NBUF - 1 && b < nmine; ++b) {
+      mbar_expect_tx(bar + b, SS::bytes);
+      bulk_load(buffer(b), gin + (first + b * step) * a.idist, SS::bytes, bar + b);
+    }
+  }
+  __syncthreads();
+  int64_t i = 0;
+  for (; i < nmine; ++i) {
+    const int b = (int)(i % NBUF);
+    const bool got = mbar_wait(bar + b, (uint32_t)((i / NBUF) & 1));
+    // every thread has also finished line i-1, so its buffer is free
+    if (!__syncthreads_and(got)) break;
+    const int64_t nx = i + NBUF - 1;
+    if (u == 0 && nx < nmine) {
+      const int bb = (int)(nx % NBUF);
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_expect_tx(bar + bb, SS::bytes);
+      bulk_load(buffer(bb), gin + (first + nx * step) * a.idist, SS::bytes, bar + bb);
+    }
+    C* buf = buffer(b);
+    const FlatIn<R> in{buf};
+    const DirectOut<R> out{gout + (first + i * step) * a.odist, true, (R)a.scale};
+    fast_prog<R, DIR, RL, T>(buf, in, out, (const C*)a.tw, (const R*)a.prime_cs, u);
+  }
+  if (i < nmine && u == 0) {
+    // gave up on line i: flag it, then let the copies still in flight land
+    if (a.err) atomicExch(a.err, kErrWaitTimeout);
+    for (int64_t k = i; k < nmine && k < i + NBUF - 1; ++k)
+      mbar_wait(bar + (int)(k % NBUF), (uint32_t)((k / NBUF) & 1));
+  }
 }
 
 // -------------------------------------------------------- tile kernel
@@ -393,6 +533,42 @@ template <typename R, class RL, int T> struct FastEntry {
     if (e != cudaSuccess) launch_failure(k, "direct launch", L, T, a.G, smem, e);
     return e;
   }
+  // Persistent launch: as many blocks as fit on the device at once (or one
+  // per line, if fewer).
+  static cudaError_t launch_stream(int dir, const FastArgs& a, cudaStream_t s) {
+    if constexpr (!StreamShape<R, RL>::ok) {
+      snprintf(g_launch_msg, sizeof(g_launch_msg), "no stream kernel for L=%d", L);
+      return cudaErrorNotSupported;
+    } else {
+      static int set_fwd[64] = {0}, set_bwd[64] = {0}, occ[2][64] = {{0}};
+      constexpr size_t smem = StreamShape<R, RL>::smem;
+      auto k = dir < 0 ? fast_stream_kernel<R, -1, RL, T> : fast_stream_kernel<R, 1, RL, T>;
+      int dev = 0;
+      cudaError_t e = cudaGetDevice(&dev);
+      if (e == cudaSuccess) e = configure(k, smem, dir < 0 ? set_fwd : set_bwd);
+      int* o = dev < 64 ? &occ[dir < 0 ? 0 : 1][dev] : nullptr;
+      int per_sm = o ? *o : 0;
+      if (e == cudaSuccess && per_sm == 0) {
+        int nsm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, T, smem);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        per_sm = per_sm * nsm;
+        if (o) *o = per_sm;
+      }
+      if (e != cudaSuccess || per_sm <= 0) {
+        if (e == cudaSuccess) e = cudaErrorInvalidConfiguration;
+        launch_failure(k, "stream set-up", L, T, 1, smem, e);
+        return e;
+      }
+      if (a.nlines <= 0) return cudaSuccess;
+      const int64_t nblk = a.nlines < per_sm ? a.nlines : per_sm;
+      k<<<dim3((unsigned)nblk), dim3(T), smem, s>>>(a);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) launch_failure(k, "stream launch", L, T, 1, smem, e);
+      return e;
+    }
+  }
+  static constexpr bool has_stream = StreamShape<R, RL>::ok;
   static cudaError_t launch_tile(const LineArgs& a, cudaStream_t s) {
     static int set_plain[64] = {0}, set_mid[64] = {0}, set_full[64] = {0};
     const size_t smem = (size_t)a.G * LPAD * sizeof(cplx<R>) + (size_t)a.G * 4 * sizeof(int64_t);

@@ -16,7 +16,10 @@ namespace fb {
   {L, T, RList<__VA_ARGS__>::n, {__VA_ARGS__},                                 \
    &FastEntry<FB_R, RList<__VA_ARGS__>, T>::launch,                            \
    &FastEntry<FB_R, RList<__VA_ARGS__>, T>::launch_tile,                       \
-   (size_t)FastEntry<FB_R, RList<__VA_ARGS__>, T>::LPAD}
+   (size_t)FastEntry<FB_R, RList<__VA_ARGS__>, T>::LPAD,                       \
+   FastEntry<FB_R, RList<__VA_ARGS__>, T>::has_stream                          \
+       ? &FastEntry<FB_R, RList<__VA_ARGS__>, T>::launch_stream                \
+       : nullptr}
 
 static const FastFn kTable[] = {
 #include "fb_fast_table.inc"

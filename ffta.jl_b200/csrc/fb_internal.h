@@ -27,7 +27,7 @@ struct LineIO {
 };
 
 // A stage program: Stockham passes with the given radices, the per-stage
-// twiddle tables at tw + tw_off[s] (entries k*(R-1) + r-1 = w_P^(r k),
+// twiddle tables at tw + tw_off[s] (entries (r-1)*Ns + k = w_P^(r k),
 // P = Ns*R, forward sign).
 struct StageProg {
   int L;
@@ -88,7 +88,12 @@ struct FastArgs {
   const int64_t* pre;
   const void* const* ins;
   void* const* outs;
+  int* err;  // device flag: kErrWaitTimeout when a bulk-copy wait gave up
 };
+
+// Value of the kernel error flag when a wait on a bulk copy gave up (after
+// about a second); the kernel then stops early and leaves its output partial.
+constexpr int kErrWaitTimeout = -1;
 
 // One specialised length: its radix program, threads per line, launcher and
 // padded shared-memory elements per line.
@@ -98,6 +103,9 @@ struct FastFn {
   cudaError_t (*launch)(int dir, const FastArgs&, cudaStream_t);
   cudaError_t (*launch_tile)(const LineArgs&, cudaStream_t);
   size_t lpad;
+  // persistent bulk-copy variant of `launch` (contiguous, 16-byte aligned
+  // lines; see fast_stream_kernel), nullptr where the length has none
+  cudaError_t (*launch_stream)(int dir, const FastArgs&, cudaStream_t);
 };
 // The compiled specialised lengths of a type (dtype 0/1), in `parts` pieces.
 int fast_table_parts();

@@ -154,8 +154,10 @@ template <typename C>
 __global__ void k_stage_tw(C* out, int R, int64_t Ns, int64_t count) {
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < count;
        idx += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t k = idx / (R - 1);
-    const int64_t r = idx % (R - 1) + 1;
+    // r-major: the R-1 twiddles of butterfly k sit Ns apart, so the threads
+    // of a warp (consecutive k) read consecutive entries
+    const int64_t r = idx / Ns + 1;
+    const int64_t k = idx % Ns;
     out[idx] = from_d2<C>(root_fp64(r * k, Ns * R));
   }
 }

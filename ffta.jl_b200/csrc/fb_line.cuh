@@ -98,9 +98,9 @@ __device__ __noinline__ void stage(cplx<R>* buf, int L, int Ns, const cplx<R>* _
     if (j < nb) {
       const int k = j % Ns;
       if (Ns > 1) {
-        const cplx<R>* w = tw + k * (RAD - 1) - 1;
+        const cplx<R>* w = tw + k;  // entry (r-1)*Ns + k
 #pragma unroll
-        for (int r = 1; r < RAD; ++r) v[q][r] = ctw<R, DIR>(v[q][r], __ldg(w + r));
+        for (int r = 1; r < RAD; ++r) v[q][r] = ctw<R, DIR>(v[q][r], __ldg(w + (r - 1) * Ns));
       }
       butterfly<R, RAD, DIR>(v[q], pcs);
       const int base = (j - k) * RAD + k;

@@ -258,6 +258,7 @@ struct Pass {
   const FastFn* fast = nullptr;    // specialised direct-I/O kernel, if any
   FastArgs fa;
   const FastFn* staged = nullptr;  // specialised tile kernel (strided lines, fused I/O)
+  int stream = 0;                  // 1: run `fast` as its persistent bulk-copy kernel
 };
 
 // The specialised kernel for a radix program, if one is compiled.
@@ -334,6 +335,7 @@ struct fb_plan_s {
 namespace fb {
 
 static int pick_G(const fb_plan_s* P, int L, int T, int Lpad, bool elem_major, int64_t nlines);
+static void apply_tuning(fb_plan_s* P);
 
 // Switch a generic pass to the compile-time tile kernel of its length when
 // one is compiled (same arithmetic, direct HBM I/O, lines fastest across a
@@ -346,11 +348,14 @@ static void use_tile(const fb_plan_s* P, Pass& p, const std::vector<int>& radice
   const int es = elem_bytes(P->dtype);
   const int T = ff->T;
   const int thr_cap = std::max(1, std::max(512, T) / T);
-  const int smem_cap = (int)std::max<size_t>(1, (100 * 1024) / ((size_t)ff->lpad * es + 32));
+  // shared memory per block: 100 KB for ComplexF32; ComplexF64 tiles run
+  // faster at about 40 KB (more resident blocks per SM, measured)
+  const size_t budget = es == 8 ? 100 * 1024 : 40 * 1024;
+  const int smem_cap = (int)std::max<size_t>(1, budget / ((size_t)ff->lpad * es + 32));
   const bool em = p.a.ld.mode == 1 || p.a.st.mode == 1;
   // strided tiles: as many neighbouring lines as the block allows (longer
-  // contiguous runs per DRAM page); contiguous lines: 256-thread blocks
-  const int want = em ? thr_cap : std::max(1, 256 / T);
+  // contiguous runs per DRAM page); contiguous lines: 128-thread blocks
+  const int want = em ? thr_cap : std::max(1, 128 / T);
   int G = std::min(std::min(thr_cap, smem_cap), want);
   const int64_t nl = std::max<int64_t>(1, p.a.nlines);
   while (G > 1 && G / 2 >= nl) G /= 2;
@@ -633,10 +638,17 @@ static Axis plan_direct_axis(fb_plan_s* P, int64_t n, LineX& x, int64_t is, int6
     p.fa.prime_cs = p.a.prime_cs;
     p.fa.scale = 1.0;
     const int es = elem_bytes(P->dtype);
-    int G = std::max(1, 256 / ff->T);  // 256-thread blocks (fb_fast.cuh DirectBounds)
+    // one line per block once a line fills a warp: measured faster than
+    // packing several lines into 256-thread blocks (fewer lines wait at each
+    // stage barrier); shorter lines share a block up to a warp's worth
+    int G = std::max(1, 32 / ff->T);
     while (G > 1 && (size_t)G * ff->lpad * es > 100 * 1024) G /= 2;
     while (G > 1 && G / 2 >= nl) G /= 2;
     p.fa.G = G;
+    p.fa.err = p.a.err;
+    // the persistent bulk-copy variant measured slower than one line per
+    // block (it holds fewer warps per SM): used on request or when tuned
+    p.stream = ff->launch_stream && (P->flags & FB_FLAG_STREAM) ? 1 : 0;
     std::ostringstream w;
     w << "FAST(L=" << x.L << " radices=";
     for (size_t i = 0; i < x.radices.size(); ++i) w << (i ? "x" : "") << x.radices[i];
@@ -1011,6 +1023,7 @@ static fb_plan_s* create_plan(int dtype, int dir, int rank, const int64_t* dims,
     if (need1) P->scratch1.reset(new DevBuf(P->scratch_elems * elem_bytes(dtype)));
   }
   cuda_check(cudaDeviceSynchronize(), "plan tables");
+  apply_tuning(P.get());
   return P.release();
 }
 
@@ -1058,7 +1071,11 @@ static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s
           fa.in = a.in;
           fa.out = a.out;
           if (last) fa.scale = P->scale;
-          const cudaError_t e = p.fast->launch(P->dir, fa, s);
+          // the bulk copies need 16-byte aligned line starts
+          const bool st = p.stream && p.fast->launch_stream &&
+                          reinterpret_cast<uintptr_t>(fa.in) % 16 == 0 && (fa.idist * es) % 16 == 0;
+          const cudaError_t e =
+              st ? p.fast->launch_stream(P->dir, fa, s) : p.fast->launch(P->dir, fa, s);
           if (e != cudaSuccess) cuda_check(e, last_launch_message());
           continue;
         }
@@ -1313,7 +1330,13 @@ int fb_plan_describe(fb_plan plan, char* buf, size_t len) {
     for (auto& ax : plan->axes) {
       o << " | n=" << ax.n << " " << ax.kind;
       if (!ax.outer.empty()) o << " (host loop " << ax.outer.size() << " dims)";
-      for (auto& p : ax.passes) o << " " << p.what;
+      for (auto& p : ax.passes) {
+        o << " " << p.what;
+        if (p.fast)
+          o << (p.stream ? "<stream>" : "<G=") << (p.stream ? "" : std::to_string(p.fa.G) + ">");
+        else
+          o << "<G=" << p.a.G << " T=" << p.a.T << " v=" << p.variant << ">";
+      }
     }
     std::string s = o.str();
     std::snprintf(buf, len, "%s", s.c_str());
@@ -1781,6 +1804,241 @@ int fb_server_destroy(fb_server srv) {
     if (!srv) return;
     cudaDeviceSynchronize();
     delete srv;
+  });
+}
+
+}  // extern "C"
+
+// ================================================================= autotuner
+// Launch shapes -- lines per block (G) of every pass and, for passes on the
+// generic kernel, its register budget (16 or 32 values per thread, which sets
+// the threads per line) -- are timed on the caller's buffers and the fastest
+// kept.  Winners are cached per plan key (type, direction, dims, strides,
+// region: i.e. per length, batch and layout) for later plans in the process,
+// and can be saved to / loaded from a text file.  The stage program of a
+// length is never tuned: it fixes the arithmetic, which must not depend on the
+// batch (batched and single transforms stay bit-identical).
+namespace fb {
+
+struct TuneEntry {
+  std::vector<int> G, T, variant;
+};
+static std::mutex g_tune_mu;
+static std::map<std::string, TuneEntry> g_tune;
+
+static std::string plan_key(const fb_plan_s* P) {
+  std::ostringstream k;
+  k << P->dtype << ":" << P->dir << ":" << P->cutoff << ":" << P->flags << ":";
+  for (int d = 0; d < P->rank; ++d)
+    k << P->dims[d] << "/" << P->istrides[d] << "/" << P->ostrides[d] << ",";
+  k << ":";
+  for (int r : P->region) k << r << ",";
+  return k.str();
+}
+
+static std::vector<Pass*> all_passes(fb_plan_s* P) {
+  std::vector<Pass*> v;
+  for (auto& ax : P->axes)
+    for (auto& p : ax.passes) v.push_back(&p);
+  return v;
+}
+
+static int& pass_G(Pass& p) { return p.fast ? p.fa.G : p.a.G; }
+
+// Candidate shapes of a pass that its kernel accepts.
+struct Shape {
+  int G, T, variant;
+};
+
+static std::vector<Shape> pass_shapes(const fb_plan_s* P, const Pass& p) {
+  // lines per block: the planner's choice and a geometric ladder around it
+  std::vector<int> gs;
+  const int G0 = p.fast ? p.fa.G : p.a.G;
+  gs.push_back(G0);
+  for (int g = 1; g <= 1024; g = g < 4 ? g + 1 : g + g / 2) gs.push_back(g);
+  std::sort(gs.begin(), gs.end());
+  gs.erase(std::unique(gs.begin(), gs.end()), gs.end());
+  std::vector<Shape> out;
+  const int es = elem_bytes(P->dtype);
+  const int64_t nl = std::max<int64_t>(1, p.fast ? p.fa.nlines : p.a.nlines);
+  const size_t smem_max = 200 * 1024;
+  if (p.fast) {
+    // variant 1: the persistent bulk-copy kernel (one line per block)
+    const int T = p.fast->T, cap = std::max(1, (T >= 256 ? T : 256) / T);
+    if (p.fast->launch_stream) out.push_back({1, T, 1});
+    for (int G : gs)
+      if (G <= cap && (G == G0 || G <= nl) && (size_t)G * p.fast->lpad * es <= smem_max)
+        out.push_back({G, T, 0});
+  } else if (p.staged) {
+    const int T = p.staged->T, cap = std::max(1, std::max(512, T) / T);
+    for (int G : gs)
+      if (G <= cap && (G == G0 || G <= nl) && (size_t)G * (p.staged->lpad * es + 32) <= smem_max)
+        out.push_back({G, T, 0});
+  } else {
+    // generic kernel: both register budgets, each with the line-count ladder
+    std::vector<int> rad(p.a.prog.radix, p.a.prog.radix + p.a.prog.nst);
+    bool big = false;
+    for (int R : rad) big |= R > 16;
+    const bool em = p.a.ld.mode == 1 || p.a.st.mode == 1;
+    for (int cap : {16, 32}) {
+      if (big && cap == 32) continue;
+      int tmin = 1;
+      for (int R : rad) tmin = std::max(tmin, (p.a.prog.L / R + um_for(R, cap) - 1) / um_for(R, cap));
+      if (tmin > line_max_threads()) continue;
+      int T = 1;
+      if (tmin <= 32) {
+        while (T < tmin) T <<= 1;
+      } else {
+        T = (tmin + 31) / 32 * 32;
+      }
+      const int variant = (cap == 32 ? 1 : 0) | (big ? 2 : 0);
+      for (int G : gs) {
+        if (em && (G & (G - 1))) continue;  // element-major tiles take powers of two
+        if (G * T > line_max_threads() || (G != G0 && G > nl)) continue;
+        LineArgs a = p.a;
+        a.G = G;
+        a.T = T;
+        if (line_smem_bytes(P->dtype, a) > smem_max) continue;
+        out.push_back({G, T, variant});
+      }
+    }
+  }
+  return out;
+}
+
+static void set_shape(Pass& p, const Shape& s) {
+  pass_G(p) = s.G;
+  if (p.fast) {
+    p.stream = s.variant;
+  } else if (!p.staged) {
+    p.a.T = s.T;
+    p.variant = s.variant;
+  }
+}
+
+static int pass_variant(const Pass& p) { return p.fast ? p.stream : p.variant; }
+
+// A cached entry is applied only when every one of its shapes is one the
+// pass's kernel accepts (a file may come from another build or be edited).
+static void apply_tuning(fb_plan_s* P) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(plan_key(P));
+  if (it == g_tune.end()) return;
+  auto ps = all_passes(P);
+  const TuneEntry& e = it->second;
+  if (ps.size() != e.G.size()) return;
+  std::vector<Shape> pick(ps.size());
+  for (size_t i = 0; i < ps.size(); ++i) {
+    const bool generic = !ps[i]->fast && !ps[i]->staged;
+    bool ok = false;
+    for (const Shape& s : pass_shapes(P, *ps[i]))
+      if (s.G == e.G[i] && s.variant == e.variant[i] && (!generic || s.T == e.T[i])) {
+        ok = true;
+        pick[i] = s;
+      }
+    if (!ok) return;
+  }
+  for (size_t i = 0; i < ps.size(); ++i) set_shape(*ps[i], pick[i]);
+}
+
+static double time_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t st, int iters) {
+  cudaEvent_t e0, e1;
+  cuda_check(cudaEventCreate(&e0), "event");
+  cuda_check(cudaEventCreate(&e1), "event");
+  execute_plan(P, in, out, st);  // warm (attributes, caches)
+  cuda_check(cudaEventRecord(e0, st), "event");
+  for (int i = 0; i < iters; ++i) execute_plan(P, in, out, st);
+  cuda_check(cudaEventRecord(e1, st), "event");
+  cuda_check(cudaEventSynchronize(e1), "event sync");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return ms / std::max(1, iters);
+}
+
+}  // namespace fb
+
+extern "C" {
+
+int fb_plan_autotune(fb_plan plan, const void* in, void* out, void* stream, int iters) {
+  return guard([&] {
+    if (!plan) fail(FB_ERR_ARGUMENT, "null plan");
+    if (plan->real_kind) fail(FB_ERR_UNSUPPORTED, "autotune a real plan through its complex plan");
+    if (plan->in_span == 0) return;
+    if (!in || !out) fail(FB_ERR_ARGUMENT, "null data pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    iters = std::max(1, iters);
+    auto ps = all_passes(plan);
+    for (Pass* p : ps) {
+      auto shapes = pass_shapes(plan, *p);
+      if (shapes.size() < 2) continue;
+      Shape best{pass_G(*p), p->a.T, pass_variant(*p)};
+      double tbest = time_plan(plan, in, out, st, iters);
+      for (const Shape& s : shapes) {
+        set_shape(*p, s);
+        const double t = time_plan(plan, in, out, st, iters);
+        if (t < tbest) {
+          tbest = t;
+          best = s;
+        }
+      }
+      set_shape(*p, best);
+    }
+    TuneEntry e;
+    for (Pass* p : ps) {
+      e.G.push_back(pass_G(*p));
+      e.T.push_back(p->a.T);
+      e.variant.push_back(pass_variant(*p));
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[plan_key(plan)] = e;
+  });
+}
+
+int fb_tune_cache_save(const char* path) {
+  return guard([&] {
+    if (!path) fail(FB_ERR_ARGUMENT, "null path");
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    FILE* f = std::fopen(path, "w");
+    if (!f) fail(FB_ERR_ARGUMENT, std::string("cannot write ") + path);
+    std::fprintf(f, "# fftab200 tuning cache v1: key|G,T,variant;...\n");
+    for (auto& kv : g_tune) {
+      std::fprintf(f, "%s|", kv.first.c_str());
+      for (size_t i = 0; i < kv.second.G.size(); ++i)
+        std::fprintf(f, "%d,%d,%d;", kv.second.G[i], kv.second.T[i], kv.second.variant[i]);
+      std::fprintf(f, "\n");
+    }
+    std::fclose(f);
+  });
+}
+
+int fb_tune_cache_load(const char* path) {
+  return guard([&] {
+    if (!path) fail(FB_ERR_ARGUMENT, "null path");
+    FILE* f = std::fopen(path, "r");
+    if (!f) fail(FB_ERR_ARGUMENT, std::string("cannot read ") + path);
+    char line[8192];
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    while (std::fgets(line, sizeof(line), f)) {
+      std::string l(line);
+      if (l.empty() || l[0] == '#') continue;
+      const size_t bar = l.find('|');
+      if (bar == std::string::npos) continue;
+      TuneEntry e;
+      std::istringstream rest(l.substr(bar + 1));
+      std::string item;
+      while (std::getline(rest, item, ';')) {
+        int G, T, v;
+        if (std::sscanf(item.c_str(), "%d,%d,%d", &G, &T, &v) == 3) {
+          e.G.push_back(G);
+          e.T.push_back(T);
+          e.variant.push_back(v);
+        }
+      }
+      g_tune[l.substr(0, bar)] = e;
+    }
+    std::fclose(f);
   });
 }
 

@@ -32,7 +32,8 @@ __all__ = [
     "FFT_FORWARD", "FFT_BACKWARD", "DEFAULT_BLUESTEIN_CUTOFF", "DimensionMismatch",
     "ArgumentError", "DomainError", "CudaError", "UnsupportedError", "FFTAPlan_cx", "plan_fft",
     "plan_bfft", "plan_ifft", "fft", "bfft", "ifft", "mul_", "size", "version", "FFTAPlan_re",
-    "plan_rfft", "plan_brfft", "plan_irfft", "rfft", "brfft", "irfft",
+    "plan_rfft", "plan_brfft", "plan_irfft", "rfft", "brfft", "irfft", "autotune",
+    "save_tuning", "load_tuning",
 ]
 
 FFT_FORWARD = -1  # src/callgraph.jl:1
@@ -315,6 +316,7 @@ def _make_plan(x, region, direction, cutoff, scale_inverse=False, flags=0):
 
 FB_FLAG_GENERIC_ONLY = 1  # include/fftab200.h: generic kernels only (for tests)
 FB_FLAG_SAME_SCHEDULE_STRIDED = 2  # strided axes bit-identical to contiguous ones
+FB_FLAG_STREAM = 4  # persistent bulk-copy kernel for contiguous lines (bit-identical)
 
 
 def plan_fft(x, region=None, *, BLUESTEIN_CUTOFF=DEFAULT_BLUESTEIN_CUTOFF, _flags=0, **_kwargs):
@@ -645,3 +647,32 @@ def irfft(x, len_, region=None, **kw):
     if not _is_torch(x):
         x = np.asarray(x)
     return plan_irfft(x, len_, region, **kw) * x
+
+
+# ------------------------------------------------------------- autotuner
+def autotune(p: FFTAPlan_cx, x, y=None, iters: int = 5):
+    """Tune the launch shapes `p` uses for arrays laid out like `x` (device
+    tensors; `y` defaults to a scratch output, and both are overwritten).
+    Later plans for the same length, type, batch and layout start from the
+    result (fb_plan_autotune).  Returns the tuned schedule's description."""
+    import torch
+    x = p._accept(x)
+    if not _is_torch(x):
+        raise ArgumentError("autotune needs device tensors")
+    if y is None:
+        y = _similar(x)
+    h = p._cplan(y, x)
+    stream = torch.cuda.current_stream(x.device).cuda_stream
+    _check(lib.fb_plan_autotune(h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(y.data_ptr()),
+                                ctypes.c_void_p(stream), int(iters)))
+    return p.describe(x)
+
+
+def save_tuning(path: str) -> None:
+    """Write the process's tuning cache to a text file."""
+    _check(lib.fb_tune_cache_save(path.encode()))
+
+
+def load_tuning(path: str) -> None:
+    """Merge a tuning cache file into the process's cache."""
+    _check(lib.fb_tune_cache_load(path.encode()))

@@ -60,6 +60,9 @@ SIGNATURES = {
     "fb_server_stats": ([_vp, _i64p, ctypes.c_int], ctypes.c_int),
     "fb_server_reset_clock": ([_vp], ctypes.c_int),
     "fb_server_destroy": ([_vp], ctypes.c_int),
+    "fb_plan_autotune": ([_vp, _vp, _vp, _vp, ctypes.c_int], ctypes.c_int),
+    "fb_tune_cache_save": ([ctypes.c_char_p], ctypes.c_int),
+    "fb_tune_cache_load": ([ctypes.c_char_p], ctypes.c_int),
     "fb_last_error": ([], ctypes.c_char_p),
     "fb_version": ([], ctypes.c_char_p),
 }

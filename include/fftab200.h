@@ -54,8 +54,15 @@ enum { FB_DEFAULT_BLUESTEIN_CUTOFF = 73 }; /* src/callgraph.jl:44 */
  *   four-step split that moves long contiguous runs; its results equal the
  *   contiguous schedule's within rounding but not bit for bit.  With the flag
  *   every strided transform is bit-identical to the same transform of a
- *   contiguous copy (FFTA's `==` property), at lower speed for those axes. */
-enum { FB_FLAG_GENERIC_ONLY = 1u, FB_FLAG_SAME_SCHEDULE_STRIDED = 2u };
+ *   contiguous copy (FFTA's `==` property), at lower speed for those axes.
+ * FB_FLAG_STREAM: run contiguous lines with the persistent bulk-copy
+ *   variant of the specialised kernel where the length has one (bit-identical
+ *   results; the autotuner also considers it). */
+enum {
+  FB_FLAG_GENERIC_ONLY = 1u,
+  FB_FLAG_SAME_SCHEDULE_STRIDED = 2u,
+  FB_FLAG_STREAM = 4u
+};
 
 /* Batched 1-D plan: `batch` transforms of length n; element j of transform b
  * is read at in[b*idist + j*istride] and written at out[b*odist + j*ostride].
@@ -188,8 +195,23 @@ int fb_plan_destroy(fb_plan plan);
 int fb_execute_noalloc_c32(const void* in, void* out, int64_t n, int64_t batch, int dir,
                            void* stream);
 
-/* Diagnostic: the current device's kernel error flag (0, or a radix that a
- * stage program named without a butterfly for it), optionally reset.  No
+/* Autotuner (no FFTA counterpart: FFTA's plans are fixed by its call graph,
+ * src/callgraph.jl:76-126).  Runs the plan `iters` times per candidate launch
+ * shape -- lines per block of each pass and, on the generic kernel, threads
+ * per line -- on the given device buffers (their contents are overwritten),
+ * keeps the fastest, and caches it for later plans of this process with the
+ * same type, direction, dims, strides and region.  The stage program of a
+ * length (its radix order) is not tuned, so results do not change. */
+int fb_plan_autotune(fb_plan plan, const void* in, void* out, void* stream, int iters);
+/* Save / load the process-wide tuning cache (a text file).  Loaded entries
+ * are applied only where every shape is valid for the plan's kernels. */
+int fb_tune_cache_save(const char* path);
+int fb_tune_cache_load(const char* path);
+
+/* Diagnostic: the current device's kernel error flag (0; a radix that a
+ * stage program named without a butterfly for it; or -1 when a kernel gave up
+ * waiting about a second for one of its bulk copies to land and stopped
+ * early, leaving that output partial), optionally reset.  No
  * FFTA counterpart: FFTA raises ArgumentError("kernel not implemented")
  * for an unknown node type (src/algos.jl:31). */
 int fb_kernel_error_flag(int* value, int reset);
