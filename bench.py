@@ -352,11 +352,16 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         nthreads = os.cpu_count() or 1
-        sample = 2048
+        sample = BATCH  # the whole batch: about 10-30 CPU-seconds on a host of 8-32 cores
         v, dt = cpu_baseline(N, sample, nthreads)
+        v1, dt1 = cpu_baseline(N, 256, 1)
         cpu = {"value": v, "unit": "GFLOP/s", "cores": nthreads, "kind": "port",
-               "sample": f"{sample} transforms of C32 N={N} (of the {BATCH}-column batch), "
-                         f"split over {nthreads} threads, {dt:.1f} s"}
+               "sample": f"{sample} transforms of C32 N={N} (the whole {BATCH}-column batch), "
+                         f"split over {nthreads} threads: {dt:.2f} s wall, "
+                         f"{dt * nthreads:.0f} thread-seconds",
+               "single_thread": {"value": v1, "unit": "GFLOP/s", "cores": 1,
+                                 "sample": f"256 transforms of N={N} on one thread "
+                                           f"(FFTA itself is single-threaded), {dt1:.2f} s"}}
 
     if rank == 0:
         wl = (f"batched C32 forward FFT, N={N}, {BATCH} contiguous columns per GPU"

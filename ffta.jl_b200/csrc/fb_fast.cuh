@@ -69,12 +69,17 @@ __host__ __device__ constexpr int lpad_of(int L) {
 // loads element i of the line / stores element i of the line.
 struct SmemIO {};
 
+// Input functors load element i in two steps: raw(i) issues the memory load,
+// fin(i, v) applies what depends on the element (tables, twiddles).  A stage
+// issues all of its raw loads before any fin, so every data load is in flight
+// before the table loads take registers.
 template <typename R> struct DirectIn {
   const cplx<R>* __restrict__ g;
   bool ok;
-  __device__ __forceinline__ cplx<R> operator()(int i) const {
+  __device__ __forceinline__ cplx<R> raw(int i) const {
     return ok ? g[i] : Sc<R>::mk(R(0), R(0));
   }
+  __device__ __forceinline__ cplx<R> fin(int, cplx<R> v) const { return v; }
 };
 template <typename R> struct DirectOut {
   cplx<R>* __restrict__ g;
@@ -96,10 +101,14 @@ template <typename R> struct TileIn {
   const cplx<R>* __restrict__ tab;  // twiddle on load (LineArgs::tw_on_load)
   int64_t tab_es, tab_off;
   int tw_dir;
-  __device__ __forceinline__ cplx<R> operator()(int i) const {
+  __device__ __forceinline__ cplx<R> raw(int i) const {
     const int64_t vi = (int64_t)i * ves + voff;
     if (!ok || vi >= vn) return Sc<R>::mk(R(0), R(0));
-    cplx<R> v = base[(int64_t)i * es];
+    return base[(int64_t)i * es];
+  }
+  __device__ __forceinline__ cplx<R> fin(int i, cplx<R> v) const {
+    const int64_t vi = (int64_t)i * ves + voff;
+    if (!ok || vi >= vn) return v;
     if (mul) v = cmul<R>(v, __ldg(mul + vi));
     if (tab) {
       const cplx<R> w = __ldg(tab + (int64_t)i * tab_es + tab_off);
@@ -149,8 +158,8 @@ template <typename R> struct PlainIn {
   int es;
   const cplx<R>* __restrict__ tab;  // twiddle on load (LineArgs::tw_on_load)
   int tab_es, tab_off, tw_dir;
-  __device__ __forceinline__ cplx<R> operator()(int i) const {
-    cplx<R> v = base[(int64_t)(i * es)];
+  __device__ __forceinline__ cplx<R> raw(int i) const { return base[(int64_t)(i * es)]; }
+  __device__ __forceinline__ cplx<R> fin(int i, cplx<R> v) const {
     if (tab) {
       const cplx<R> w = __ldg(tab + (i * tab_es + tab_off));
       v = tw_dir < 0 ? cmul<R>(v, w) : cmulc<R>(v, w);
@@ -180,7 +189,8 @@ template <typename R> struct PlainOut {
 // same buffer in the padded layout, after a barrier.
 template <typename R> struct FlatIn {
   const cplx<R>* p;
-  __device__ __forceinline__ cplx<R> operator()(int i) const { return p[i]; }
+  __device__ __forceinline__ cplx<R> raw(int i) const { return p[i]; }
+  __device__ __forceinline__ cplx<R> fin(int, cplx<R> v) const { return v; }
 };
 template <class In> struct InIsSmem : std::false_type {};
 template <typename R> struct InIsSmem<FlatIn<R>> : std::true_type {};
@@ -208,9 +218,19 @@ __device__ __forceinline__ void fast_stage(cplx<R>* buf, const In& in, const Out
 #pragma unroll
       for (int r = 0; r < RAD; ++r) {
         if constexpr (GIN)
-          v[q][r] = in(j + r * nb);
+          v[q][r] = in.raw(j + r * nb);
         else
           v[q][r] = buf[padi(j + r * nb)];
+      }
+    }
+  }
+  if constexpr (GIN) {
+#pragma unroll
+    for (int q = 0; q < UM; ++q) {
+      const int j = u + q * T;
+      if (nb % T == 0 || j < nb) {
+#pragma unroll
+        for (int r = 0; r < RAD; ++r) v[q][r] = in.fin(j + r * nb, v[q][r]);
       }
     }
   }
