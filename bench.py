@@ -330,6 +330,42 @@ def main():
                 "schedule": pe.describe(xj)}
             del xe, ye, pe, xj, yj
 
+    # configuration 4: 2-D ComplexF32 with the plain FP32 path and with the
+    # split-BF16 tensor-core radix-16 stage, rel-L2 vs the FP64 oracle for each
+    precision = {}
+    if not args.no_extra and rank == 0 and not args.workload:
+        import oracle
+        for plabel, pdims in (("c32_2d_4096x4096", (4096, 4096)), ("c32_2d_2187x2048", (2187, 2048)),
+                              ("c32_2d_1000x1000", (1000, 1000))):
+            gen = torch.Generator(device=dev).manual_seed(4)
+            xr = torch.complex(torch.randn(tuple(reversed(pdims)), device=dev, generator=gen),
+                               torch.randn(tuple(reversed(pdims)), device=dev, generator=gen))
+            xj = xr.permute(1, 0)
+            yj = torch.empty_like(xr).permute(1, 0)
+            ref = oracle.fft_nd(xj.cpu().numpy().astype(np.complex128), [1, 2], -1, prec="f64",
+                                nthreads=os.cpu_count() or 1)
+            row = {}
+            for name, fl in (("fp32", 0), ("tensor_stage", F.FB_FLAG_TENSOR_STAGE)):
+                pp = F.plan_fft(xj, (1, 2), _flags=fl)
+                for _ in range(3):
+                    F.mul_(yj, pp, xj)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(10):
+                    F.mul_(yj, pp, xj)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                t = e0.elapsed_time(e1) / 10
+                y = yj.cpu().numpy()
+                en = int(np.prod(pdims))
+                row[name] = {"ms": t, "GB/s": 2.0 * en * 8 / (t * 1e-3) / 1e9,
+                             "rel_l2_vs_fp64_oracle": float(np.linalg.norm(y - ref) /
+                                                            np.linalg.norm(ref)),
+                             "tensor_core_passes": pp.describe(xj).count("<tc>"),
+                             "schedule": pp.describe(xj)}
+            precision[plabel] = row
+            del xr, xj, yj
+
     serving_out = None
     if rank == 0 and world == 1 and not args.no_serving and not args.workload:
         from ffta_b200 import serving as S
@@ -389,6 +425,7 @@ def main():
             "cpu_baseline": cpu,
             "extra": extra,
             "serving": serving_out,
+            "config4_precision": precision or None,
         }
         print(json.dumps(line))
     if world > 1:

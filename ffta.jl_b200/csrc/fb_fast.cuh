@@ -29,6 +29,7 @@
 #include <type_traits>
 
 #include "fb_line.cuh"
+#include "fb_tc.cuh"
 
 namespace fb {
 
@@ -200,9 +201,12 @@ template <typename R> struct InIsSmem<FlatIn<R>> : std::true_type {};
 // of T owns butterflies j = u + q*T.  The first stage takes its inputs from
 // `in` unless it is SmemIO; the last stage gives its outputs to `out` unless
 // it is SmemIO.
-template <typename R, int DIR, class RL, int S, int T, class In, class Out>
+// TC: stage 0 is the radix-16 DFT on the tensor cores (tc::tc_dft16, context
+// *tcx) instead of the FP32 butterfly.
+template <typename R, int DIR, class RL, int S, int T, class In, class Out, bool TC = false>
 __device__ __forceinline__ void fast_stage(cplx<R>* buf, const In& in, const Out& out,
-                                           const cplx<R>* __restrict__ tw, const R* pcs, int u) {
+                                           const cplx<R>* __restrict__ tw, const R* pcs, int u,
+                                           const tc::TcCtx* tcx = nullptr) {
   constexpr int L = prog_len<RL>();
   constexpr int RAD = RL::r[S];
   constexpr int Ns = ns_before<RL, S>();
@@ -210,6 +214,8 @@ __device__ __forceinline__ void fast_stage(cplx<R>* buf, const In& in, const Out
   constexpr int UM = (nb + T - 1) / T;
   constexpr bool GIN = S == 0 && !std::is_same<In, SmemIO>::value;
   constexpr bool GOUT = S == RL::n - 1 && !std::is_same<Out, SmemIO>::value;
+  static_assert(!TC || (S == 0 && RAD == 16 && UM == 1 && nb == T && std::is_same<R, float>::value),
+                "the tensor-core stage is a first radix-16 stage, one butterfly per thread");
   cplx<R> v[UM][RAD];
 #pragma unroll
   for (int q = 0; q < UM; ++q) {
@@ -247,7 +253,10 @@ __device__ __forceinline__ void fast_stage(cplx<R>* buf, const In& in, const Out
 #pragma unroll
         for (int r = 1; r < RAD; ++r) v[q][r] = ctw<R, DIR>(v[q][r], __ldg(w + (r - 1) * Ns));
       }
-      butterfly<R, RAD, DIR>(v[q], pcs);
+      if constexpr (TC)
+        tc::tc_dft16(v[q], *tcx);
+      else
+        butterfly<R, RAD, DIR>(v[q], pcs);
       const int base = (j - k) * RAD + k;
 #pragma unroll
       for (int r = 0; r < RAD; ++r) {
@@ -261,11 +270,13 @@ __device__ __forceinline__ void fast_stage(cplx<R>* buf, const In& in, const Out
   if constexpr (!GOUT) __syncthreads();
 }
 
-template <typename R, int DIR, class RL, int T, class In, class Out, int S = 0>
+template <typename R, int DIR, class RL, int T, class In, class Out, int S = 0, bool TC = false>
 __device__ __forceinline__ void fast_prog(cplx<R>* buf, const In& in, const Out& out,
-                                          const cplx<R>* tw, const R* pcs, int u) {
-  fast_stage<R, DIR, RL, S, T, In, Out>(buf, in, out, tw, pcs, u);
-  if constexpr (S + 1 < RL::n) fast_prog<R, DIR, RL, T, In, Out, S + 1>(buf, in, out, tw, pcs, u);
+                                          const cplx<R>* tw, const R* pcs, int u,
+                                          const tc::TcCtx* tcx = nullptr) {
+  fast_stage<R, DIR, RL, S, T, In, Out, TC && S == 0>(buf, in, out, tw, pcs, u, tcx);
+  if constexpr (S + 1 < RL::n)
+    fast_prog<R, DIR, RL, T, In, Out, S + 1, TC>(buf, in, out, tw, pcs, u, tcx);
 }
 
 // ------------------------------------------------------ direct kernel
@@ -319,53 +330,6 @@ __global__ void __launch_bounds__(DirectBounds<R, T>::threads, DirectBounds<R, T
 // that of the other kernels.  Every wait is bounded: after about a second the
 // block sets kErrWaitTimeout, waits (again bounded) for its copies in flight
 // and returns.
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t* b, int count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(count)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(b)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(done)
-      : "r"(smem_addr(b)), "r"(parity)
-      : "memory");
-  return done != 0;
-}
-__device__ __forceinline__ uint64_t global_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-// Wait for phase `parity` of *b for at most ~1 s; false if it gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
-  if (mbar_test(b, parity)) return true;
-  const uint64_t t0 = global_ns();
-  for (uint32_t it = 0; it < (1u << 30); ++it) {
-    if (mbar_test(b, parity)) return true;
-    if ((it & 63) == 63 && global_ns() - t0 > 1000000000ull) return false;
-  }
-  return false;
-}
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
-                                          uint64_t* b) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-          "r"(smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(b))
-      : "memory");
-}
 
 template <typename R, class RL> struct StreamShape {
   static constexpr int L = prog_len<RL>();
@@ -505,6 +469,110 @@ __global__ void __launch_bounds__(T > 512 ? T : 512) fast_tile_kernel(const Line
   }
 }
 
+// ------------------------------------------------ tensor-core variants
+// The direct kernel and the lean-I/O tile kernel with their first radix-16
+// stage on the tensor cores (tc::tc_dft16).  Shared memory: the stage's A
+// operand and the line buffers share the first region (lines are written
+// only after the products complete), then (tile kernel) the per-line
+// offsets, the B table, the mbarrier and the tensor-memory address.
+template <class RL, int T> struct TcShape {
+  static constexpr int L = prog_len<RL>();
+  static constexpr size_t line_bytes = (size_t)lpad_of(L) * 8;
+  static constexpr bool first16 = RL::r[0] == 16 && L / 16 == T;  // one butterfly per thread
+  static constexpr bool direct_ok = first16 && T % 128 == 0 && T <= 512;
+  static constexpr bool tile_ok = first16 && T <= 512 && 512 % T == 0;
+  __host__ __device__ static constexpr size_t region(int G) {
+    return ((((size_t)G * line_bytes > (size_t)G * T * tc::kTcRowBytes)
+                 ? (size_t)G * line_bytes
+                 : (size_t)G * T * tc::kTcRowBytes) +
+            127) / 128 * 128;
+  }
+  __host__ __device__ static constexpr size_t direct_smem() {
+    return region(1) + tc::kTcTableBytes + 16;
+  }
+  __host__ __device__ static constexpr size_t tile_smem(int G) {
+    return region(G) + (size_t)G * 32 + tc::kTcTableBytes + 16;
+  }
+  static constexpr int direct_blocks =
+      (int)(232448 / (direct_smem() + 1024)) < 1 ? 1 : (int)(232448 / (direct_smem() + 1024));
+};
+
+template <int DIR, class RL, int T>
+__global__ void __launch_bounds__(T, TcShape<RL, T>::direct_blocks)
+    fast_tc_direct_kernel(const FastArgs a) {
+  typedef cplx<float> C;
+  typedef TcShape<RL, T> TS;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  unsigned char* b = smraw + TS::region(1);
+  uint64_t* bar = (uint64_t*)(b + tc::kTcTableBytes);
+  uint32_t* slot = (uint32_t*)(bar + 1);
+  const int u = threadIdx.x;
+  const tc::TcCtx c =
+      tc::tc_begin(smraw, b, bar, slot,
+                   (const unsigned char*)a.tcb + (DIR < 0 ? 0 : tc::kTcTableBytes), a.err, u, T);
+  const int64_t line = blockIdx.x;  // grid = lines
+  const DirectIn<float> in{(const C*)a.in + line * a.idist, true};
+  const DirectOut<float> out{(C*)a.out + line * a.odist, true, (float)a.scale};
+  fast_prog<float, DIR, RL, T, DirectIn<float>, DirectOut<float>, 0, true>(
+      (C*)smraw, in, out, (const C*)a.tw, (const float*)a.prime_cs, u, &c);
+  tc::tc_end(c);
+}
+
+template <class RL, int T>
+__global__ void __launch_bounds__(512, 2) fast_tc_tile_kernel(const LineArgs a) {
+  typedef cplx<float> C;
+  typedef TcShape<RL, T> TS;
+  constexpr int LPAD = lpad_of(prog_len<RL>());
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int g = threadIdx.x, u = threadIdx.y, G = a.G;
+  const size_t reg = TS::region(G);
+  int64_t* lb = (int64_t*)(smraw + reg);
+  unsigned char* b = smraw + reg + (size_t)G * 32;
+  uint64_t* bar = (uint64_t*)(b + tc::kTcTableBytes);
+  uint32_t* slot = (uint32_t*)(bar + 1);
+  C* buf = (C*)smraw + g * LPAD;
+  const int64_t line = (int64_t)blockIdx.x * G + g;
+  const bool ok = line < a.nlines;
+  if (u == 0) {
+    const int64_t l = ok ? line : 0;
+    const int64_t q0 = l % a.m0, t = l / a.m0;
+    const int64_t q1 = t % a.m1, q2 = t / a.m1;
+    lb[4 * g + 1] = q0 * a.ld.s0 + q1 * a.ld.s1 + q2 * a.ld.s2;
+    lb[4 * g + 2] = q0 * a.st.s0 + q1 * a.st.s1 + q2 * a.st.s2;
+    lb[4 * g + 3] = a.tw_level ? q1 : q0;
+  }
+  // (tc_begin's barrier publishes lb)
+  const tc::TcCtx c = tc::tc_begin(
+      smraw, b, bar, slot, (const unsigned char*)a.tcb + (a.dir1 < 0 ? 0 : tc::kTcTableBytes),
+      a.err, g + G * u, G * T);
+  const int64_t lt = lb[4 * g + 3];
+  const C* tin = a.tw_on_load ? (const C*)a.tw_tab : nullptr;
+  const C* tout = a.tw_on_load ? nullptr : (const C*)a.tw_tab;
+  const PlainIn<float> in{(const C*)a.in + lb[4 * g + 1], (int)a.ld.es, tin, (int)a.tw_es,
+                          (int)(lt * a.tw_ls), a.tw_dir};
+  const PlainOut<float> out{(C*)a.out + lb[4 * g + 2], (int)a.st.es, tout, (int)a.tw_es,
+                            (int)(lt * a.tw_ls), a.tw_dir, (float)a.scale, ok};
+  const C* tw = (const C*)a.prog.tw;
+  const float* pcs = (const float*)a.prime_cs;
+  if (a.dir1 < 0)
+    fast_prog<float, -1, RL, T, PlainIn<float>, PlainOut<float>, 0, true>(buf, in, out, tw, pcs,
+                                                                          u, &c);
+  else
+    fast_prog<float, 1, RL, T, PlainIn<float>, PlainOut<float>, 0, true>(buf, in, out, tw, pcs,
+                                                                         u, &c);
+  tc::tc_end(c);
+}
+
+// Refuse a tensor-core launch whose resident blocks could ask for more than
+// the SM's 512 tensor-memory columns (an allocation would then wait).
+template <typename K> static cudaError_t tc_check_columns(K k, int threads, size_t smem, uint32_t cols) {
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem);
+  if (e != cudaSuccess) return e;
+  return (per_sm >= 1 && (uint32_t)per_sm * cols <= 512u) ? cudaSuccess
+                                                          : cudaErrorInvalidConfiguration;
+}
+
 // ---------------------------------------------------------- launching
 // Raise a kernel's dynamic shared-memory limit when a launch needs more than
 // the default 48 KB.  `set` is the caller's per-kernel, per-device record.
@@ -589,6 +657,56 @@ template <typename R, class RL, int T> struct FastEntry {
     }
   }
   static constexpr bool has_stream = StreamShape<R, RL>::ok;
+  static constexpr bool has_tc = std::is_same<R, float>::value && TcShape<RL, T>::direct_ok;
+  static constexpr bool has_tile_tc = std::is_same<R, float>::value && TcShape<RL, T>::tile_ok;
+  static cudaError_t launch_tc(int dir, const FastArgs& a, cudaStream_t s) {
+    if constexpr (!has_tc) {
+      snprintf(g_launch_msg, sizeof(g_launch_msg), "no tensor-core stage for L=%d", L);
+      return cudaErrorNotSupported;
+    } else {
+      static int set_fwd[64] = {0}, set_bwd[64] = {0};
+      constexpr size_t smem = TcShape<RL, T>::direct_smem();
+      auto k = dir < 0 ? fast_tc_direct_kernel<-1, RL, T> : fast_tc_direct_kernel<1, RL, T>;
+      cudaError_t e = configure(k, smem, dir < 0 ? set_fwd : set_bwd);
+      if (e == cudaSuccess) e = tc_check_columns(k, T, smem, tc::tc_cols(T));
+      if (e != cudaSuccess) {
+        launch_failure(k, "tensor-core direct set-up", L, T, 1, smem, e);
+        return e;
+      }
+      if (a.nlines <= 0) return cudaSuccess;
+      k<<<dim3((unsigned)a.nlines), dim3(T), smem, s>>>(a);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) launch_failure(k, "tensor-core direct launch", L, T, 1, smem, e);
+      return e;
+    }
+  }
+  static cudaError_t launch_tile_tc(const LineArgs& a, cudaStream_t s) {
+    if constexpr (!has_tile_tc) {
+      snprintf(g_launch_msg, sizeof(g_launch_msg), "no tensor-core tile stage for L=%d", L);
+      return cudaErrorNotSupported;
+    } else {
+      static int set[64] = {0};
+      const size_t smem = TcShape<RL, T>::tile_smem(a.G);
+      auto k = fast_tc_tile_kernel<RL, T>;
+      const int nt = a.G * T;
+      if (nt % 128 != 0 || nt > 512 || a.mid || !a.plain_io) {
+        launch_failure(k, "tensor-core tile shape", L, T, a.G, smem, cudaErrorInvalidValue);
+        return cudaErrorInvalidValue;
+      }
+      cudaError_t e = configure(k, smem, set);
+      if (e == cudaSuccess) e = tc_check_columns(k, nt, smem, tc::tc_cols(nt));
+      if (e != cudaSuccess) {
+        launch_failure(k, "tensor-core tile set-up", L, T, a.G, smem, e);
+        return e;
+      }
+      const int64_t nblk = (a.nlines + a.G - 1) / a.G;
+      if (nblk <= 0) return cudaSuccess;
+      k<<<dim3((unsigned)nblk), dim3(a.G, T), smem, s>>>(a);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) launch_failure(k, "tensor-core tile launch", L, T, a.G, smem, e);
+      return e;
+    }
+  }
   static cudaError_t launch_tile(const LineArgs& a, cudaStream_t s) {
     static int set_plain[64] = {0}, set_mid[64] = {0}, set_full[64] = {0};
     const size_t smem = (size_t)a.G * LPAD * sizeof(cplx<R>) + (size_t)a.G * 4 * sizeof(int64_t);

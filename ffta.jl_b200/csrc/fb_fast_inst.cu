@@ -19,6 +19,12 @@ namespace fb {
    (size_t)FastEntry<FB_R, RList<__VA_ARGS__>, T>::LPAD,                       \
    FastEntry<FB_R, RList<__VA_ARGS__>, T>::has_stream                          \
        ? &FastEntry<FB_R, RList<__VA_ARGS__>, T>::launch_stream                \
+       : nullptr,                                                              \
+   FastEntry<FB_R, RList<__VA_ARGS__>, T>::has_tc                              \
+       ? &FastEntry<FB_R, RList<__VA_ARGS__>, T>::launch_tc                    \
+       : nullptr,                                                              \
+   FastEntry<FB_R, RList<__VA_ARGS__>, T>::has_tile_tc                         \
+       ? &FastEntry<FB_R, RList<__VA_ARGS__>, T>::launch_tile_tc               \
        : nullptr}
 
 static const FastFn kTable[] = {

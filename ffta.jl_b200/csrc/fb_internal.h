@@ -68,6 +68,7 @@ struct LineArgs {
   const void* prime_cs; // cos/sin tables of odd primes (see prime_table_offset)
   int* err;             // device flag: set to the radix when a program names one
                         // this kernel has no butterfly for (never traps)
+  const void* tcb;      // tensor-core stage: B tables (forward, then backward)
 };
 
 // Arguments of the specialised direct-I/O kernel (fb_fast.cuh): `nlines`
@@ -89,6 +90,7 @@ struct FastArgs {
   const void* const* ins;
   void* const* outs;
   int* err;  // device flag: kErrWaitTimeout when a bulk-copy wait gave up
+  const void* tcb;  // tensor-core stage: B tables (forward, then backward)
 };
 
 // Value of the kernel error flag when a wait on a bulk copy gave up (after
@@ -106,7 +108,14 @@ struct FastFn {
   // persistent bulk-copy variant of `launch` (contiguous, 16-byte aligned
   // lines; see fast_stream_kernel), nullptr where the length has none
   cudaError_t (*launch_stream)(int dir, const FastArgs&, cudaStream_t);
+  // the same kernels with the first radix-16 stage on the tensor cores
+  // (split-BF16 GEMM, FP32 accumulation); nullptr where not available
+  cudaError_t (*launch_tc)(int dir, const FastArgs&, cudaStream_t);
+  cudaError_t (*launch_tile_tc)(const LineArgs&, cudaStream_t);
 };
+
+// Bytes of one direction's B table of the tensor-core radix-16 stage.
+constexpr int kTcTableBytesHost = 6144;
 // The compiled specialised lengths of a type (dtype 0/1), in `parts` pieces.
 int fast_table_parts();
 const FastFn* fast_table(int dtype, int part, int* count);

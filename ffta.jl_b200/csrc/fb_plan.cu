@@ -73,6 +73,7 @@ struct DeviceTables {
   void* f32 = nullptr;
   void* f64 = nullptr;
   int* err = nullptr;  // kernel error flag (see LineArgs::err)
+  void* tc = nullptr;  // B tables of the tensor-core radix-16 stage (made on first use)
 };
 static std::mutex g_dev_mu;
 static std::map<int, DeviceTables> g_dev_tables;
@@ -90,6 +91,79 @@ static const DeviceTables& device_tables(int dev) {
   cuda_check(gen_prime_tables(t.f32, t.f64, 0), "prime tables");
   cuda_check(cudaDeviceSynchronize(), "prime tables");
   return g_dev_tables.emplace(dev, t).first->second;
+}
+
+// Round to nearest even FP32 -> BF16 (finite inputs).
+static uint16_t bf16_bits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  u += 0x7FFFu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+static double bf16_value(uint16_t b) {
+  const uint32_t u = (uint32_t)b << 16;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+// B operand of the tensor-core radix-16 stage for both directions (forward
+// table, then backward): row o < 16 gives Re y_o = sum_n Re(F_on) re_n -
+// Im(F_on) im_n, row 16+o gives Im y_o = sum_n Im(F_on) re_n + Re(F_on) im_n,
+// F_on = exp(dir 2 pi i (o n mod 16) / 16); each entry split into three BF16
+// terms (h, m, l: residuals of the FP64 value) in column blocks 0-31, 32-63,
+// 64-95, stored in the K-major canonical shared-memory layout.
+static const void* tc_tables(int dev) {
+  static std::mutex mu;
+  static std::map<int, void*> made;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = made.find(dev);
+  if (it != made.end()) return it->second;
+  const int K = 96;
+  std::vector<uint16_t> host(2 * kTcTableBytesHost / 2, 0);
+  // cos(pi m / 8) for m = 0..15 with exact zeros and ones
+  auto cos8 = [](int m) -> double {
+    m &= 15;
+    if (m == 0) return 1.0;
+    if (m == 8) return -1.0;
+    if (m == 4 || m == 12) return 0.0;
+    return std::cos(M_PI * m / 8.0);
+  };
+  for (int d = 0; d < 2; ++d) {
+    const int dir = d == 0 ? -1 : 1;
+    uint16_t* tab = host.data() + d * (kTcTableBytesHost / 2);
+    for (int o = 0; o < 32; ++o) {
+      const int k = o & 15;
+      for (int c = 0; c < 32; ++c) {
+        const int n = c & 15;
+        const int m = (k * n) & 15;
+        const double fr = cos8(m), fi = dir * cos8(m + 12);  // sin(pi m/8) = cos(pi (m-4)/8)
+        double val;
+        if (o < 16)
+          val = c < 16 ? fr : -fi;
+        else
+          val = c < 16 ? fi : fr;
+        const uint16_t h = bf16_bits((float)val);
+        const double r1 = val - bf16_value(h);
+        const uint16_t mm = bf16_bits((float)r1);
+        const double r2 = r1 - bf16_value(mm);
+        const uint16_t l = bf16_bits((float)r2);
+        const uint16_t parts[3] = {h, mm, l};
+        for (int blk = 0; blk < 3; ++blk) {
+          const int kk = blk * 32 + c;
+          const size_t off = (size_t)((o >> 3) * (K / 8) * 128 + (kk >> 3) * 128 + (o & 7) * 16 +
+                                      (kk & 7) * 2);
+          tab[off / 2] = parts[blk];
+        }
+      }
+    }
+  }
+  void* p = nullptr;
+  cuda_check(cudaMalloc(&p, 2 * kTcTableBytesHost), "cudaMalloc");
+  cuda_check(cudaMemcpy(p, host.data(), 2 * kTcTableBytesHost, cudaMemcpyHostToDevice),
+             "tensor-core tables");
+  made[dev] = p;
+  return p;
 }
 
 // ------------------------------------------------------------ arithmetic
@@ -259,6 +333,7 @@ struct Pass {
   FastArgs fa;
   const FastFn* staged = nullptr;  // specialised tile kernel (strided lines, fused I/O)
   int stream = 0;                  // 1: run `fast` as its persistent bulk-copy kernel
+  int tc = 0;                      // 1: first radix-16 stage on the tensor cores
 };
 
 // The specialised kernel for a radix program, if one is compiled.
@@ -371,6 +446,12 @@ static void use_tile(const fb_plan_s* P, Pass& p, const std::vector<int>& radice
   p.a.plain_io = !p.a.mid && !p.a.ld.mul && !p.a.st.mul && p.a.ld.vn == INT64_MAX &&
                  p.a.st.vn == INT64_MAX && !(p.a.tw_N && !p.a.tw_tab) && small &&
                  p.a.ld.count == L && p.a.st.count == L;
+  if ((P->flags & FB_FLAG_TENSOR_STAGE) && ff->launch_tile_tc && p.a.plain_io) {
+    // 512 threads per block: four 128-row tiles of the stage's GEMM
+    p.tc = 1;
+    p.a.G = 512 / T;
+    p.a.tcb = tc_tables(P->device);
+  }
   p.what += "[tile T=" + std::to_string(T) + " G=" + std::to_string(p.a.G) + "]";
 }
 
@@ -646,6 +727,11 @@ static Axis plan_direct_axis(fb_plan_s* P, int64_t n, LineX& x, int64_t is, int6
     while (G > 1 && G / 2 >= nl) G /= 2;
     p.fa.G = G;
     p.fa.err = p.a.err;
+    if ((P->flags & FB_FLAG_TENSOR_STAGE) && ff->launch_tc) {
+      p.tc = 1;
+      p.fa.G = 1;
+      p.fa.tcb = tc_tables(P->device);
+    }
     // the persistent bulk-copy variant measured slower than one line per
     // block (it holds fewer warps per SM): used on request or when tuned
     p.stream = ff->launch_stream && (P->flags & FB_FLAG_STREAM) ? 1 : 0;
@@ -1074,14 +1160,15 @@ static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s
           // the bulk copies need 16-byte aligned line starts
           const bool st = p.stream && p.fast->launch_stream &&
                           reinterpret_cast<uintptr_t>(fa.in) % 16 == 0 && (fa.idist * es) % 16 == 0;
-          const cudaError_t e =
-              st ? p.fast->launch_stream(P->dir, fa, s) : p.fast->launch(P->dir, fa, s);
+          const cudaError_t e = p.tc ? p.fast->launch_tc(P->dir, fa, s)
+                                : st ? p.fast->launch_stream(P->dir, fa, s)
+                                     : p.fast->launch(P->dir, fa, s);
           if (e != cudaSuccess) cuda_check(e, last_launch_message());
           continue;
         }
         if (last && P->scale != 1.0) a.scale = P->scale * a.scale;
         if (p.staged) {
-          const cudaError_t e = p.staged->launch_tile(a, s);
+          const cudaError_t e = p.tc ? p.staged->launch_tile_tc(a, s) : p.staged->launch_tile(a, s);
           if (e != cudaSuccess) cuda_check(e, last_launch_message());
           continue;
         }
@@ -1332,7 +1419,9 @@ int fb_plan_describe(fb_plan plan, char* buf, size_t len) {
       if (!ax.outer.empty()) o << " (host loop " << ax.outer.size() << " dims)";
       for (auto& p : ax.passes) {
         o << " " << p.what;
-        if (p.fast)
+        if (p.tc)
+          o << "<tc>";
+        else if (p.fast)
           o << (p.stream ? "<stream>" : "<G=") << (p.stream ? "" : std::to_string(p.fa.G) + ">");
         else
           o << "<G=" << p.a.G << " T=" << p.a.T << " v=" << p.variant << ">";
@@ -1851,6 +1940,7 @@ struct Shape {
 };
 
 static std::vector<Shape> pass_shapes(const fb_plan_s* P, const Pass& p) {
+  if (p.tc) return {};  // the tensor-core stage fixes its block shape
   // lines per block: the planner's choice and a geometric ladder around it
   std::vector<int> gs;
   const int G0 = p.fast ? p.fa.G : p.a.G;

@@ -57,11 +57,18 @@ enum { FB_DEFAULT_BLUESTEIN_CUTOFF = 73 }; /* src/callgraph.jl:44 */
  *   contiguous copy (FFTA's `==` property), at lower speed for those axes.
  * FB_FLAG_STREAM: run contiguous lines with the persistent bulk-copy
  *   variant of the specialised kernel where the length has one (bit-identical
- *   results; the autotuner also considers it). */
+ *   results; the autotuner also considers it).
+ * FB_FLAG_TENSOR_STAGE: ComplexF32 only -- compute the first radix-16 stage
+ *   of each specialised pass whose program starts with 16 on the tensor cores
+ *   (tcgen05, split-BF16 operands in three terms, FP32 accumulation) instead
+ *   of the FP32 butterflies.  Error stays at the FP32 path's level; results
+ *   are not bit-identical to the default path.  No FFTA counterpart (FFTA
+ *   computes in the element type only). */
 enum {
   FB_FLAG_GENERIC_ONLY = 1u,
   FB_FLAG_SAME_SCHEDULE_STRIDED = 2u,
-  FB_FLAG_STREAM = 4u
+  FB_FLAG_STREAM = 4u,
+  FB_FLAG_TENSOR_STAGE = 8u
 };
 
 /* Batched 1-D plan: `batch` transforms of length n; element j of transform b
