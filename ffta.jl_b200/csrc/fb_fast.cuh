@@ -154,15 +154,17 @@ template <typename R> struct TileOut {
 // Lean I/O for the common case (LineArgs::plain_io): every element present,
 // no chirp tables, 32-bit strides, twiddle (if any) from a full table.  The
 // line index is clamped to a valid line, so loads need no predicate.
+// `tab` is a generic pointer: the twiddle table in global memory, or the
+// line's slice of it staged in shared memory (then tab_es = 1, tab_off = 0).
 template <typename R> struct PlainIn {
   const cplx<R>* __restrict__ base;
   int es;
-  const cplx<R>* __restrict__ tab;  // twiddle on load (LineArgs::tw_on_load)
+  const cplx<R>* tab;  // twiddle on load (LineArgs::tw_on_load)
   int tab_es, tab_off, tw_dir;
   __device__ __forceinline__ cplx<R> raw(int i) const { return base[(int64_t)(i * es)]; }
   __device__ __forceinline__ cplx<R> fin(int i, cplx<R> v) const {
     if (tab) {
-      const cplx<R> w = __ldg(tab + (i * tab_es + tab_off));
+      const cplx<R> w = tab[i * tab_es + tab_off];
       v = tw_dir < 0 ? cmul<R>(v, w) : cmulc<R>(v, w);
     }
     return v;
@@ -171,13 +173,13 @@ template <typename R> struct PlainIn {
 template <typename R> struct PlainOut {
   cplx<R>* __restrict__ base;
   int es;
-  const cplx<R>* __restrict__ tab;
+  const cplx<R>* tab;
   int tab_es, tab_off, tw_dir;
   R scale;
   bool ok;
   __device__ __forceinline__ void operator()(int i, cplx<R> v) const {
     if (tab) {
-      const cplx<R> w = __ldg(tab + (i * tab_es + tab_off));
+      const cplx<R> w = tab[i * tab_es + tab_off];
       v = tw_dir < 0 ? cmul<R>(v, w) : cmulc<R>(v, w);
     }
     if (scale != R(1)) v = cscale<R>(v, scale);
@@ -403,44 +405,90 @@ __global__ void __launch_bounds__(T, StreamBounds<R, RL, T>::min_blocks)
 }
 
 // -------------------------------------------------------- tile kernel
+// Most complex values one thread holds in any stage of program RL on T threads.
+template <class RL, int T> __host__ __device__ constexpr int max_values() {
+  int m = 0;
+  for (int i = 0; i < RL::n; ++i) {
+    const int nb = prog_len<RL>() / RL::r[i];
+    const int v = (nb + T - 1) / T * RL::r[i];
+    m = v > m ? v : m;
+  }
+  return m;
+}
+template <typename R, class RL, int T, bool MID, bool PLAIN> struct TileBounds {
+  static constexpr int min_blocks =
+      (sizeof(R) == 4 && PLAIN && !MID && T <= 512 && max_values<RL, T>() <= 18) ? 2 : 1;
+};
+// Whether a tile launch reserves shared memory for a staged twiddle slice:
+// only four-step passes whose slice follows the second batch level.
+__host__ __device__ inline bool stages_twiddles(const LineArgs& a, int L) {
+  return a.tw_tab && a.tw_level == 1 && L <= kStagedTwiddleMax;
+}
+// Lines of one block that share their twiddle slice (four-step passes over a
+// contiguous batch: the slice depends on the line's second batch level only)
+// read it from shared memory: stage entries tab[i*tw_es + lt*tw_ls], i < L,
+// into `dst` when the block's first and last lines agree on lt.  Returns dst,
+// or nullptr (and stages nothing) otherwise.  Every thread calls it.
+template <typename C>
+__device__ __forceinline__ const C* stage_twiddles(const LineArgs& a, const int64_t* lt_of,
+                                                   int G, int L, C* dst, int tid, int nthreads) {
+  if (!stages_twiddles(a, L)) return nullptr;
+  const int64_t left = a.nlines - (int64_t)blockIdx.x * G;
+  const int last = (int)(left < G ? left : G) - 1;
+  const int64_t lt = lt_of[0];
+  if (lt_of[last] != lt) return nullptr;
+  const C* __restrict__ tab = (const C*)a.tw_tab + lt * a.tw_ls;
+  for (int i = tid; i < L; i += nthreads) dst[i] = __ldg(tab + (int64_t)i * a.tw_es);
+  __syncthreads();
+  return dst;
+}
+
 // G lines per block addressed like the generic kernel (LineArgs: three batch
 // levels, element strides, presence window, tables).  Thread (g, u) is
 // threadIdx.x = g, threadIdx.y = u, so a warp spans 32/G butterflies of G
 // lines.  MID: forward program, multiply by a.mid, inverse program.
 template <typename R, class RL, int T, bool MID, bool PLAIN>
-__global__ void __launch_bounds__(T > 512 ? T : 512) fast_tile_kernel(const LineArgs a) {
+// ComplexF32 lean-I/O blocks of up to 512 threads are held to 64 registers
+// so two fit per SM (measured faster than one block with more registers),
+// unless a thread holds more than 18 values in some stage.
+__global__ void __launch_bounds__(T > 512 ? T : 512, TileBounds<R, RL, T, MID, PLAIN>::min_blocks)
+    fast_tile_kernel(const LineArgs a) {
   typedef cplx<R> C;
   constexpr int L = prog_len<RL>();
   constexpr int LPAD = lpad_of(L);
   extern __shared__ __align__(16) unsigned char smraw[];
   const int g = threadIdx.x, u = threadIdx.y;
-  C* buf = (C*)smraw + g * LPAD;
+  const int G = a.G, P = tile_pitch(LPAD, G, (int)sizeof(C));
+  C* buf = (C*)smraw + g * P;
   // one thread per line splits its index into the batch levels (64-bit
   // divisions) and leaves the results in shared memory for the others
-  int64_t* lb = (int64_t*)((C*)smraw + (size_t)a.G * LPAD);
-  const int64_t line = (int64_t)blockIdx.x * a.G + g;
+  // (four arrays of G entries, so a warp's reads are consecutive)
+  int64_t* lb = (int64_t*)((C*)smraw + (size_t)G * P);
+  const int64_t line = (int64_t)blockIdx.x * G + g;
   const bool ok = line < a.nlines;
   if (u == 0) {
     const int64_t l = ok ? line : 0;
     const int64_t q0 = l % a.m0, t = l / a.m0;
     const int64_t q1 = t % a.m1, q2 = t / a.m1;
-    lb[4 * g + 0] = q0;
-    lb[4 * g + 1] = q0 * a.ld.s0 + q1 * a.ld.s1 + q2 * a.ld.s2;
-    lb[4 * g + 2] = q0 * a.st.s0 + q1 * a.st.s1 + q2 * a.st.s2;
-    lb[4 * g + 3] = a.tw_level ? q1 : q0;
+    lb[g] = q0;
+    lb[G + g] = q0 * a.ld.s0 + q1 * a.ld.s1 + q2 * a.ld.s2;
+    lb[2 * G + g] = q0 * a.st.s0 + q1 * a.st.s1 + q2 * a.st.s2;
+    lb[3 * G + g] = a.tw_level ? q1 : q0;
   }
   __syncthreads();
-  const int64_t l0 = lb[4 * g + 0], lt = lb[4 * g + 3];
+  const int64_t l0 = lb[g], lt = lb[3 * G + g];
   const C* tw = (const C*)a.prog.tw;
   const R* pcs = (const R*)a.prime_cs;
-  const C* ib = (const C*)a.in + lb[4 * g + 1];
-  C* ob = (C*)a.out + lb[4 * g + 2];
+  const C* ib = (const C*)a.in + lb[G + g];
+  C* ob = (C*)a.out + lb[2 * G + g];
   if constexpr (PLAIN && !MID) {
     const C* tin = a.tw_on_load ? (const C*)a.tw_tab : nullptr;
     const C* tout = a.tw_on_load ? nullptr : (const C*)a.tw_tab;
-    const PlainIn<R> in{ib, (int)a.ld.es, tin, (int)a.tw_es, (int)(lt * a.tw_ls), a.tw_dir};
-    const PlainOut<R> out{ob, (int)a.st.es, tout, (int)a.tw_es, (int)(lt * a.tw_ls), a.tw_dir,
-                          (R)a.scale, ok};
+    const C* st = stage_twiddles<C>(a, lb + 3 * G, G, L, (C*)(lb + 4 * G), g + G * u, G * T);
+    const int tes = st ? 1 : (int)a.tw_es, toff = st ? 0 : (int)(lt * a.tw_ls);
+    const PlainIn<R> in{ib, (int)a.ld.es, tin ? (st ? st : tin) : nullptr, tes, toff, a.tw_dir};
+    const PlainOut<R> out{ob, (int)a.st.es, tout ? (st ? st : tout) : nullptr, tes, toff,
+                          a.tw_dir, (R)a.scale, ok};
     if (a.dir1 < 0)
       fast_prog<R, -1, RL, T>(buf, in, out, tw, pcs, u);
     else
@@ -477,21 +525,23 @@ __global__ void __launch_bounds__(T > 512 ? T : 512) fast_tile_kernel(const Line
 // offsets, the B table, the mbarrier and the tensor-memory address.
 template <class RL, int T> struct TcShape {
   static constexpr int L = prog_len<RL>();
-  static constexpr size_t line_bytes = (size_t)lpad_of(L) * 8;
+  __host__ __device__ static constexpr size_t line_bytes(int G) {
+    return (size_t)tile_pitch(lpad_of(L), G, 8) * 8;
+  }
   static constexpr bool first16 = RL::r[0] == 16 && L / 16 == T;  // one butterfly per thread
   static constexpr bool direct_ok = first16 && T % 128 == 0 && T <= 512;
   static constexpr bool tile_ok = first16 && T <= 512 && 512 % T == 0;
   __host__ __device__ static constexpr size_t region(int G) {
-    return ((((size_t)G * line_bytes > (size_t)G * T * tc::kTcRowBytes)
-                 ? (size_t)G * line_bytes
+    return ((((size_t)G * line_bytes(G) > (size_t)G * T * tc::kTcRowBytes)
+                 ? (size_t)G * line_bytes(G)
                  : (size_t)G * T * tc::kTcRowBytes) +
             127) / 128 * 128;
   }
   __host__ __device__ static constexpr size_t direct_smem() {
     return region(1) + tc::kTcTableBytes + 16;
   }
-  __host__ __device__ static constexpr size_t tile_smem(int G) {
-    return region(G) + (size_t)G * 32 + tc::kTcTableBytes + 16;
+  __host__ __device__ static constexpr size_t tile_smem(int G, bool staged) {
+    return region(G) + (size_t)G * 32 + tc::kTcTableBytes + 16 + (staged ? (size_t)L * 8 : 0);
   }
   static constexpr int direct_blocks =
       (int)(232448 / (direct_smem() + 1024)) < 1 ? 1 : (int)(232448 / (direct_smem() + 1024));
@@ -530,28 +580,32 @@ __global__ void __launch_bounds__(512, 2) fast_tc_tile_kernel(const LineArgs a) 
   unsigned char* b = smraw + reg + (size_t)G * 32;
   uint64_t* bar = (uint64_t*)(b + tc::kTcTableBytes);
   uint32_t* slot = (uint32_t*)(bar + 1);
-  C* buf = (C*)smraw + g * LPAD;
+  C* buf = (C*)smraw + g * tile_pitch(LPAD, G, 8);
   const int64_t line = (int64_t)blockIdx.x * G + g;
   const bool ok = line < a.nlines;
   if (u == 0) {
     const int64_t l = ok ? line : 0;
     const int64_t q0 = l % a.m0, t = l / a.m0;
     const int64_t q1 = t % a.m1, q2 = t / a.m1;
-    lb[4 * g + 1] = q0 * a.ld.s0 + q1 * a.ld.s1 + q2 * a.ld.s2;
-    lb[4 * g + 2] = q0 * a.st.s0 + q1 * a.st.s1 + q2 * a.st.s2;
-    lb[4 * g + 3] = a.tw_level ? q1 : q0;
+    lb[G + g] = q0 * a.ld.s0 + q1 * a.ld.s1 + q2 * a.ld.s2;
+    lb[2 * G + g] = q0 * a.st.s0 + q1 * a.st.s1 + q2 * a.st.s2;
+    lb[3 * G + g] = a.tw_level ? q1 : q0;
   }
   // (tc_begin's barrier publishes lb)
   const tc::TcCtx c = tc::tc_begin(
       smraw, b, bar, slot, (const unsigned char*)a.tcb + (a.dir1 < 0 ? 0 : tc::kTcTableBytes),
       a.err, g + G * u, G * T);
-  const int64_t lt = lb[4 * g + 3];
+  const int64_t lt = lb[3 * G + g];
   const C* tin = a.tw_on_load ? (const C*)a.tw_tab : nullptr;
   const C* tout = a.tw_on_load ? nullptr : (const C*)a.tw_tab;
-  const PlainIn<float> in{(const C*)a.in + lb[4 * g + 1], (int)a.ld.es, tin, (int)a.tw_es,
-                          (int)(lt * a.tw_ls), a.tw_dir};
-  const PlainOut<float> out{(C*)a.out + lb[4 * g + 2], (int)a.st.es, tout, (int)a.tw_es,
-                            (int)(lt * a.tw_ls), a.tw_dir, (float)a.scale, ok};
+  const C* st = stage_twiddles<C>(a, lb + 3 * G, G, prog_len<RL>(), (C*)(slot + 2), g + G * u,
+                                  G * T);
+  const int tes = st ? 1 : (int)a.tw_es, toff = st ? 0 : (int)(lt * a.tw_ls);
+  const PlainIn<float> in{(const C*)a.in + lb[G + g], (int)a.ld.es,
+                          tin ? (st ? st : tin) : nullptr, tes, toff, a.tw_dir};
+  const PlainOut<float> out{(C*)a.out + lb[2 * G + g], (int)a.st.es,
+                            tout ? (st ? st : tout) : nullptr, tes, toff, a.tw_dir,
+                            (float)a.scale, ok};
   const C* tw = (const C*)a.prog.tw;
   const float* pcs = (const float*)a.prime_cs;
   if (a.dir1 < 0)
@@ -686,7 +740,7 @@ template <typename R, class RL, int T> struct FastEntry {
       return cudaErrorNotSupported;
     } else {
       static int set[64] = {0};
-      const size_t smem = TcShape<RL, T>::tile_smem(a.G);
+      const size_t smem = TcShape<RL, T>::tile_smem(a.G, stages_twiddles(a, L));
       auto k = fast_tc_tile_kernel<RL, T>;
       const int nt = a.G * T;
       if (nt % 128 != 0 || nt > 512 || a.mid || !a.plain_io) {
@@ -709,7 +763,9 @@ template <typename R, class RL, int T> struct FastEntry {
   }
   static cudaError_t launch_tile(const LineArgs& a, cudaStream_t s) {
     static int set_plain[64] = {0}, set_mid[64] = {0}, set_full[64] = {0};
-    const size_t smem = (size_t)a.G * LPAD * sizeof(cplx<R>) + (size_t)a.G * 4 * sizeof(int64_t);
+    const size_t smem = (size_t)a.G * tile_pitch(LPAD, a.G, (int)sizeof(cplx<R>)) * sizeof(cplx<R>) +
+                        (size_t)a.G * 4 * sizeof(int64_t) +
+                        (stages_twiddles(a, L) ? (size_t)L * sizeof(cplx<R>) : 0);
     const bool mid = a.mid != nullptr;
     auto k = mid ? fast_tile_kernel<R, RL, T, true, false>
                  : (a.plain_io ? fast_tile_kernel<R, RL, T, false, true>

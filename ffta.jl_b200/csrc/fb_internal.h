@@ -71,6 +71,20 @@ struct LineArgs {
   const void* tcb;      // tensor-core stage: B tables (forward, then backward)
 };
 
+// Shared-memory pitch (elements) of the lines of a tile block.  A warp holds
+// G lines x 32/G butterflies, and a 128-byte row of shared memory has
+// S = 128/es element slots (16 for ComplexF32, 8 for ComplexF64), served to S
+// consecutive lanes at a time.  Those lanes hit distinct slots when
+// pitch = S/G (mod S) for G < S (lines interleave with the consecutive
+// butterflies) and pitch = 1 (mod S) for G >= S (S lines side by side).
+__host__ __device__ constexpr int tile_pitch(int lpad, int G, int es) {
+  return lpad + ((((G >= 128 / es ? 1 : (128 / es) / G) - lpad) % (128 / es)) + (128 / es)) %
+                    (128 / es);
+}
+
+// Longest line whose twiddle slice a tile block stages in shared memory.
+constexpr int kStagedTwiddleMax = 1024;
+
 // Arguments of the specialised direct-I/O kernel (fb_fast.cuh): `nlines`
 // contiguous lines of length L, line l at in + l*idist / out + l*odist.
 struct FastArgs {

@@ -426,7 +426,7 @@ static void use_tile(const fb_plan_s* P, Pass& p, const std::vector<int>& radice
   // shared memory per block: 100 KB for ComplexF32; ComplexF64 tiles run
   // faster at about 40 KB (more resident blocks per SM, measured)
   const size_t budget = es == 8 ? 100 * 1024 : 40 * 1024;
-  const int smem_cap = (int)std::max<size_t>(1, budget / ((size_t)ff->lpad * es + 32));
+  const int smem_cap = (int)std::max<size_t>(1, budget / ((size_t)(ff->lpad + 15) * es + 32));
   const bool em = p.a.ld.mode == 1 || p.a.st.mode == 1;
   // strided tiles: as many neighbouring lines as the block allows (longer
   // contiguous runs per DRAM page); contiguous lines: 128-thread blocks
@@ -849,7 +849,7 @@ static Axis plan_four_axis(fb_plan_s* P, int64_t N, int64_t N1, int64_t N2, Line
   // the twiddle w_N^(n2 k1) multiplies the columns' outputs; with a full
   // table it is applied as pass 2 loads them (element n2 of line k1), so its
   // table loads issue with the data loads
-  if ((int64_t)N <= kFullTwiddle && x2.kind == 0) {
+  if ((int64_t)N <= kFullTwiddle && x2.kind == 0 && !tmode) {
     attach_twiddle(P, &p2.a, N, P->dir, N2, N1);
     p2.a.tw_on_load = 1;
     p2.a.tw_level = tmode ? 1 : 0;
@@ -1962,7 +1962,8 @@ static std::vector<Shape> pass_shapes(const fb_plan_s* P, const Pass& p) {
   } else if (p.staged) {
     const int T = p.staged->T, cap = std::max(1, std::max(512, T) / T);
     for (int G : gs)
-      if (G <= cap && (G == G0 || G <= nl) && (size_t)G * (p.staged->lpad * es + 32) <= smem_max)
+      if (G <= cap && (G == G0 || G <= nl) &&
+          (size_t)G * (tile_pitch((int)p.staged->lpad, G, es) * es + 32) <= smem_max)
         out.push_back({G, T, 0});
   } else {
     // generic kernel: both register budgets, each with the line-count ladder
