@@ -184,6 +184,9 @@ def main():
     ap.add_argument("--batch", type=int, default=BATCH,
                     help="columns per GPU (smaller for profiling captures)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving comparison")
+    ap.add_argument("--tensor-stage", action="store_true",
+                    help="time the main workload with the split-BF16 tensor-core radix-16 "
+                         "stage (ComplexF32 programs that start with 16)")
     ap.add_argument("--workload", default=None,
                     help="time one of the `extra` configurations instead of the headline "
                          "(for profiling captures): " + ", ".join(e[0] for e in EXTRA))
@@ -231,7 +234,8 @@ def main():
     y = torch.empty_like(x)
     perm = tuple(range(x.ndim - 1, -1, -1))
     xt, yt = x.permute(perm), y.permute(perm)
-    p = F.plan_fft(xt, tuple(range(1, len(dims) + 1)))
+    flags = F.FB_FLAG_TENSOR_STAGE if args.tensor_stage else 0
+    p = F.plan_fft(xt, tuple(range(1, len(dims) + 1)), _flags=flags)
     n_tot = int(np.prod(dims))
     stream = torch.cuda.current_stream(dev)
 
@@ -282,7 +286,7 @@ def main():
     hx = x.cpu().pin_memory()
     hy = torch.empty_like(hx).pin_memory()
     hxn, hyn = hx.numpy(), hy.numpy()
-    ph = F.plan_fft(hxn.T, tuple(range(1, len(dims) + 1)))
+    ph = F.plan_fft(hxn.T, tuple(range(1, len(dims) + 1)), _flags=flags)
 
     def e2e_step():
         F.mul_(hyn.T, ph, hxn.T)
