@@ -1552,12 +1552,20 @@ extern "C" int fb_plan_create_real(fb_plan* plan, int dtype, int dir, int rank,
 // ones finish.
 namespace fb {
 
+// Descriptor-launch shape of a single-pass template plan: its line
+// arguments with the thread shape and shared-memory class filled in.
+struct SrvShape {
+  LineArgs a;
+  int var = 0, threads = 0, cls = 0, G = 1;
+};
+
 struct SrvReq {
   int64_t ticket, n, batch;
   int dtype, dir;
   const void* in;
   void* out;
   double bytes;
+  const SrvShape* shape;  // nullptr: multi-pass length
 };
 
 struct SrvLaunch {
@@ -1590,7 +1598,9 @@ struct fb_server_s {
   std::vector<fb::SrvSlot> slots;
   double admitted = 0;
   int64_t next_ticket = 0;
-  std::vector<std::pair<int64_t, double>> done;
+  std::deque<std::pair<int64_t, double>> done;
+  // per template plan: its descriptor launch shape, computed once
+  std::map<const fb_plan_s*, fb::SrvShape> shapes;
   int64_t st_launches = 0, st_desc_launches = 0, st_requests = 0, st_max_queue = 0;
   double st_max_admitted = 0;
   ~fb_server_s() {
@@ -1669,9 +1679,37 @@ static void srv_retire(fb_server_s* S, bool block) {
 // Shared-memory classes of descriptor launches (bytes per block).
 static const size_t kSmemClass[4] = {16u << 10, 48u << 10, 100u << 10, 220u << 10};
 
+// The descriptor-launch shape of template T (made once per template).
+static const SrvShape* srv_shape(fb_server_s* S, const fb_plan_s* T, int dtype) {
+  auto it = S->shapes.find(T);
+  if (it != S->shapes.end()) return &it->second;
+  const Pass& p = T->axes[0].passes[0];
+  SrvShape sh;
+  sh.a = p.a;
+  int Tt = sh.a.T, var = p.variant;
+  std::vector<int> rad(sh.a.prog.radix, sh.a.prog.radix + sh.a.prog.nst);
+  if (!pick_threads(sh.a.prog.L, rad, &Tt, &var)) fail(FB_ERR_UNSUPPORTED, "no thread shape");
+  sh.threads = Tt > 256 ? 512 : 256;
+  const size_t line_bytes = (size_t)sh.a.Lpad * elem_bytes(dtype) + 4 * sizeof(int64_t);
+  int cls = 0;
+  while (cls < 3 && line_bytes > kSmemClass[cls]) ++cls;
+  int G = std::max(1, sh.threads / Tt);
+  while (G > 1 && (size_t)G * line_bytes > kSmemClass[cls]) --G;
+  sh.a.T = Tt;
+  sh.a.G = G;
+  sh.var = var;
+  sh.cls = cls;
+  sh.G = G;
+  return &(S->shapes[T] = sh);
+}
+
+// Requests one dispatch takes at most: a burst is cut into several launches
+// so building the next one's descriptors overlaps the GPU running this one.
+static const size_t kDispatchMax = 384;
+
 static void srv_dispatch(fb_server_s* S) {
   std::vector<SrvReq> batch;
-  while (!S->pending.empty()) {
+  while (!S->pending.empty() && batch.size() < kDispatchMax) {
     const SrvReq& r = S->pending.front();
     if (S->admitted + r.bytes > S->budget && (S->admitted > 0 || !batch.empty())) break;
     S->admitted += r.bytes;
@@ -1690,8 +1728,7 @@ static void srv_dispatch(fb_server_s* S) {
   };
   std::map<std::tuple<int, int, int, int>, Group> groups;
   for (const SrvReq& r : batch) {
-    fb_plan_s* T = srv_template(S, r.n, r.dtype, r.dir);
-    if (!srv_single_pass(T)) {
+    if (!r.shape) {
       fb_plan_s* P = srv_multi(S, r.n, r.dtype, r.dir, r.batch);
       execute_plan(P, r.in, r.out, S->serial);
       SrvLaunch l;
@@ -1704,20 +1741,11 @@ static void srv_dispatch(fb_server_s* S) {
       S->st_launches += 1;
       continue;
     }
-    const Pass& p = T->axes[0].passes[0];
-    LineArgs a = p.a;
-    int Tt = a.T, var = p.variant;
-    std::vector<int> rad(a.prog.radix, a.prog.radix + a.prog.nst);
-    if (!pick_threads(a.prog.L, rad, &Tt, &var)) fail(FB_ERR_UNSUPPORTED, "no thread shape");
-    const int threads = Tt > 256 ? 512 : 256;
-    const size_t es = elem_bytes(r.dtype);
-    const size_t line_bytes = (size_t)a.Lpad * es + 4 * sizeof(int64_t);
-    int cls = 0;
-    while (cls < 3 && line_bytes > kSmemClass[cls]) ++cls;
-    int G = std::max(1, threads / Tt);
-    while (G > 1 && (size_t)G * line_bytes > kSmemClass[cls]) --G;
+    const SrvShape& sh = *r.shape;
+    LineArgs a = sh.a;
+    const int var = sh.var, threads = sh.threads, cls = sh.cls;
+    int G = sh.G;
     while (G > 1 && G / 2 >= r.batch) G /= 2;
-    a.T = Tt;
     a.G = G;
     a.in = r.in;
     a.out = r.out;
@@ -1730,7 +1758,7 @@ static void srv_dispatch(fb_server_s* S) {
     g.bstart.push_back(g.bstart.back() + (r.batch + G - 1) / G);
     g.tickets.push_back(r.ticket);
     g.bytes += r.bytes;
-    g.smem = std::max(g.smem, line_smem_bytes(r.dtype, a));
+    g.smem = std::max(g.smem, line_smem_bytes(r.dtype, sh.a));
   }
   for (auto& kv : groups) {
     Group& g = kv.second;
@@ -1822,8 +1850,9 @@ int fb_server_submit(fb_server srv, int64_t n, int dtype, int dir, int64_t batch
     // plans are made at submission (tables resident); bytes = data + scratch
     fb_plan_s* T = srv_template(srv, n, dtype, dir);
     double bytes = 2.0 * (double)n * (double)batch * elem_bytes(dtype);
-    if (!srv_single_pass(T)) bytes += (double)plan_scratch_bytes(srv_multi(srv, n, dtype, dir, batch));
-    SrvReq r{srv->next_ticket++, n, batch, dtype, dir, in, out, bytes};
+    const SrvShape* shape = srv_single_pass(T) ? srv_shape(srv, T, dtype) : nullptr;
+    if (!shape) bytes += (double)plan_scratch_bytes(srv_multi(srv, n, dtype, dir, batch));
+    SrvReq r{srv->next_ticket++, n, batch, dtype, dir, in, out, bytes, shape};
     srv->pending.push_back(r);
     srv->st_requests += 1;
     srv->st_max_queue = std::max<int64_t>(srv->st_max_queue, (int64_t)srv->pending.size());
