@@ -434,6 +434,10 @@ static void use_tile(const fb_plan_s* P, Pass& p, const std::vector<int>& radice
   int G = std::min(std::min(thr_cap, smem_cap), want);
   const int64_t nl = std::max<int64_t>(1, p.a.nlines);
   while (G > 1 && G / 2 >= nl) G /= 2;
+  // lines contiguous on load: at least about four blocks per SM when the
+  // batch is small (strided loads keep their width for long DRAM runs)
+  if (p.a.ld.mode == 0)
+    while (G > 1 && nl / G < 4 * 148) G /= 2;
   p.staged = ff;
   p.a.T = T;
   p.a.G = std::max(1, G);
@@ -610,11 +614,12 @@ static void attach_blue(fb_plan_s* P, const LineX& x, LineArgs* a) {
 // (one coalesced load per element: entry i*n_ln + lt) is made; beyond, the
 // two-level tables (hi[e >> shift] * lo[e & mask]).
 static const int64_t kFullTwiddle = int64_t(1) << 23;
+static const int64_t kBlueFullTwiddle = int64_t(1) << 18;
 
 static void attach_twiddle(fb_plan_s* P, LineArgs* a, int64_t N, int dir, int64_t n_el,
-                           int64_t n_ln) {
+                           int64_t n_ln, bool roots_only = false) {
   a->tw_dir = dir;
-  if (n_el * n_ln <= kFullTwiddle) {
+  if (n_el * n_ln <= kFullTwiddle && !roots_only) {
     void* tab = alloc_table(P, (size_t)(n_el * n_ln) * elem_bytes(P->dtype));
     cuda_check(gen_tw_table(P->dtype, tab, N, n_el, n_ln, 0), "twiddle table");
     a->tw_tab = tab;
@@ -914,7 +919,11 @@ static Axis plan_blue3_axis(fb_plan_s* P, int64_t N, int64_t is, int64_t os,
   p1.a.ld.ves = M2;
   p1.a.ld.vls = 1;
   p1.a.st = io_plain(1, M, B0 * M, M2, (int)M1);
-  if (M > kFullTwiddle) attach_twiddle(P, &p1.a, M, FB_FORWARD, M1, M2);
+  // Pads above kBlueFullTwiddle take their twiddles from two small root
+  // tables on the passes' stores: a full table would be read from HBM as
+  // often as the data itself when the batch is small.
+  const bool full_tw = M <= kBlueFullTwiddle;
+  if (!full_tw) attach_twiddle(P, &p1.a, M, FB_FORWARD, M1, M2, true);
   p1.a.ld.mode = is == 1 ? 1 : 0;
   p1.a.st.mode = 1;
   p1.a.G = pick_G(P, x1.L, x1.T, p1.a.Lpad, true, p1.a.nlines);
@@ -934,12 +943,13 @@ static Axis plan_blue3_axis(fb_plan_s* P, int64_t N, int64_t is, int64_t os,
   p2.a.mid_es = M1;
   p2.a.dir1 = FB_FORWARD;
   p2.a.dir2 = FB_BACKWARD;
-  if (M <= kFullTwiddle) {
+  if (full_tw) {
     // pass 1's twiddle w_M^(n2 k1), applied as pass 2 loads (element n2 of line k1)
     attach_twiddle(P, &p2.a, M, FB_FORWARD, M2, M1);
     p2.a.tw_on_load = 1;
+  } else {
+    attach_twiddle(P, &p2.a, M, FB_BACKWARD, M2, M1, true);
   }
-  if (M > kFullTwiddle) attach_twiddle(P, &p2.a, M, FB_BACKWARD, M2, M1);
   p2.a.ld.mode = 0;
   p2.a.st.mode = 1;
   p2.a.G = pick_G(P, x2.L, x2.T, p2.a.Lpad, true, p2.a.nlines);
@@ -960,7 +970,7 @@ static Axis plan_blue3_axis(fb_plan_s* P, int64_t N, int64_t is, int64_t os,
   p3.a.st.vls = 1;
   p3.a.ld.mode = 0;
   p3.a.st.mode = os == 1 ? 1 : 0;
-  if (M <= kFullTwiddle) {
+  if (full_tw) {
     // the conjugate twiddle of pass 2's outputs, applied as pass 3 loads them
     // (element k1 of line m2)
     attach_twiddle(P, &p3.a, M, FB_BACKWARD, M1, M2);
