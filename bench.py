@@ -403,6 +403,15 @@ def main():
                                  "sample": f"256 transforms of N={N} on one thread "
                                            f"(FFTA itself is single-threaded), {dt1:.2f} s"}}
 
+    # DRAM bytes per launch of the headline kernel from one ncu capture of the
+    # same kernel at batch 4096 (profiles/fast_direct_c32_n4096.md: 134.27 MB
+    # read + 84.74 MB written), scaled by 16384/4096; writes still in L2 when
+    # that launch ended are not counted there
+    traffic, traffic_note = None, None
+    if label == "headline" and batch == 16384 and not args.tensor_stage:
+        traffic = 4 * (134.27e6 + 84.74e6)
+        traffic_note = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the batch-4096 "
+                        "launch, scaled x4 (profiles/fast_direct_c32_n4096.md)")
     if rank == 0:
         wl = (f"batched C32 forward FFT, N={N}, {BATCH} contiguous columns per GPU"
               if label == "headline" else f"{label} forward FFT")
@@ -417,7 +426,8 @@ def main():
                        "schedule": p.describe(xt)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
-                         "alg_bytes_per_launch": alg_bytes, "traffic": None},
+                         "alg_bytes_per_launch": alg_bytes, "traffic": traffic,
+                         "traffic_source": traffic_note},
             "hbm_gbs": achieved,
             "rel_l2_vs_fp64_oracle": rel,
             "e2e": {"value": e2e_value, "unit": "GFLOP/s",
