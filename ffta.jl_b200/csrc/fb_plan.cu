@@ -8,12 +8,14 @@
 //   DIRECT  one kernel: the whole line in shared memory (lengths up to Lmax)
 //   BLUE1   one kernel: Bluestein with the pad held in shared memory
 //   FOUR    two kernels: N = N1*N2, each pass a DIRECT or BLUE1 line
-//           transform, the twiddle fused into the first pass's store
+//           transform, the twiddle fused into the second pass's loads (or,
+//           over a contiguous batch, the first pass's stores)
 //   BLUE3   three kernels: Bluestein whose pad M = M1*M2 is done four-step,
 //           with the chirp spectrum multiply fused between the two halves
 // The arithmetic of a length depends only on (length, type, direction,
-// cutoff), never on batch or strides, so strided and batched transforms are
-// bit-identical to single contiguous ones.
+// cutoff), never on batch or strides, so batched transforms and strided
+// one-pass axes are bit-identical to single contiguous ones (long strided
+// axes take a four-step split unless FB_FLAG_SAME_SCHEDULE_STRIDED is set).
 #include <cuda_runtime.h>
 
 #include <algorithm>
