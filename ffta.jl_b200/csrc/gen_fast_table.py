@@ -3,6 +3,7 @@
 Each entry's radix list is the planner's radix program for that length
 (fb_plan.cu radix_program: radix 16 with a trailing 8*4 / 4 / 8 / 2 for powers
 of two, radix 9 with a trailing 3 for powers of three, then 5s and odd primes)
+for the lengths below (powers of two and three, 2^a*3, 2^a*9, 5-smooth 5^c*2^a)
 and T = L / (largest radix) threads per line (at most 512; 1024 for 16384).
 Entries are spread over PARTS compilation units so they build in parallel.
 
@@ -47,6 +48,11 @@ def lengths():
     for a in range(4, 13):
         out.add(2 ** a * 3)
         out.add(2 ** a * 9)
+    # 5-smooth lengths (2-D and four-step factors such as 1000 = 25 x 40)
+    for c in (2, 3, 4):
+        for a in range(0, 6):
+            out.add(5 ** c * 2 ** a)
+    out.add(40)
     out.add(1000)
     return sorted(x for x in out if x <= 16384)
 

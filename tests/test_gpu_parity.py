@@ -161,7 +161,7 @@ def test_twiddle_accuracy_bounds(N, bound):
 
 
 FAST_LENGTHS = [2, 4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096, 8192, 16384, 3, 9, 27, 81,
-                243, 729, 2187, 6561, 1000]
+                243, 729, 2187, 6561, 1000, 25, 40, 125, 200, 625, 800, 5000]
 
 
 @pytest.mark.parametrize("n", FAST_LENGTHS)
