@@ -194,6 +194,9 @@ static bool is_prime(int64_t n) {
 }
 static int elem_bytes(int dtype) { return dtype == FB_C32 ? 8 : 16; }
 static int64_t lmax_for(int dtype) { return dtype == FB_C32 ? 16384 : 8192; }
+// Longest contiguous ComplexF32 line done in one pass by a specialised kernel
+// (the line and its padding fill up to 167 KB of shared memory).
+static const int64_t kLongDirectMax = 19683;
 
 // ------------------------------------------------------ line transforms
 // A transform of one line done by one kernel.
@@ -1072,6 +1075,22 @@ static Axis plan_axis(fb_plan_s* P, int64_t n, int64_t is, int64_t os, std::vect
   // Bluestein for a prime in one kernel when its pad fits.
   if (is_prime(n) && make_blue1(n, P->dtype, &x))
     return plan_direct_axis(P, n, x, is, os, bd, src, dst);
+  // Contiguous ComplexF32 lines beyond the generic kernel's limit that still
+  // fit one SM's shared memory: one pass on their specialised kernel.
+  if (P->dtype == FB_C32 && n > lmax_for(FB_C32) && n <= kLongDirectMax && is == 1 && os == 1 &&
+      bd.size() <= 1 && !(P->flags & FB_FLAG_GENERIC_ONLY)) {
+    LineX lx;
+    lx.kind = 0;
+    lx.n = n;
+    lx.L = (int)n;
+    lx.radices = radix_program(n);
+    const FastFn* ff = find_fast(P->dtype, lx.L, lx.radices);
+    if (ff && ff->launch) {
+      lx.T = ff->T;
+      lx.variant = 0;
+      return plan_direct_axis(P, n, lx, is, os, bd, src, dst);
+    }
+  }
   // Four-step over the cheapest split into two one-kernel line transforms.
   double best = 1e300;
   int64_t bN1 = 0;

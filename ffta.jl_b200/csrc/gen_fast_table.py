@@ -4,7 +4,7 @@ Each entry's radix list is the planner's radix program for that length
 (fb_plan.cu radix_program: radix 16 with a trailing 8*4 / 4 / 8 / 2 for powers
 of two, radix 9 with a trailing 3 for powers of three, then 5s and odd primes)
 for the lengths below (powers of two and three, 2^a*3, 2^a*9, 5-smooth 5^c*2^a)
-and T = L / (largest radix) threads per line (at most 512; 1024 for 16384).
+and T = L / (largest radix) threads per line (at most 512; 1024 from 16384 up).
 Entries are spread over PARTS compilation units so they build in parallel.
 
 Run:  python gen_fast_table.py   (rewrites fb_fast_table.inc next to it)
@@ -54,7 +54,11 @@ def lengths():
             out.add(5 ** c * 2 ** a)
     out.add(40)
     out.add(1000)
-    return sorted(x for x in out if x <= 16384)
+    out = {x for x in out if x <= 16384}
+    # ComplexF32 lines beyond the generic kernel's limit that still fit one
+    # SM's shared memory (1024 threads per line)
+    out.add(3 ** 9)
+    return sorted(out)
 
 
 def main():
@@ -66,7 +70,7 @@ def main():
         T = L // max(rad)
         if L == 16384:
             T = 1024
-        T = min(T, 1024 if L == 16384 else 512)
+        T = min(T, 1024 if L >= 16384 else 512)
         wide = L * 16 > 8192 * 16  # longer than the ComplexF64 line limit
         ents.append((L, T, rad, wide))
     for part in range(PARTS):
