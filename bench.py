@@ -154,7 +154,7 @@ def run_reference(args):
     tot = float(np.sum(times))
     value = flops(N, sample) * args.steps / tot / 1e9
     line = {
-        "impl": "reference", "metric": "batched FFT GFLOP/s (5 N log2 N), C32 N=4096",
+        "impl": "reference", "metric": "batched FFT GFLOP/s (5 N log2 N), C32 N=4096 x 16384",
         "value": value, "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
