@@ -1919,7 +1919,16 @@ int fb_server_create(fb_server* srv, double budget_bytes, int nstreams, uint32_t
       S->streams.push_back(st);
     }
     cuda_check(cudaStreamCreateWithFlags(&S->serial, cudaStreamNonBlocking), "stream");
+    // descriptor slots sized for the largest dispatch up front: growing one
+    // later frees device memory (which synchronises the device) and
+    // allocates pinned memory in the middle of serving
     S->slots.resize(4 * ns);
+    const size_t slot_bytes = kDispatchMax * sizeof(LineArgs) + (kDispatchMax + 1) * sizeof(int64_t);
+    for (SrvSlot& sl : S->slots) {
+      sl.buf.reset(new DevBuf(slot_bytes));
+      cuda_check(cudaMallocHost(&sl.host, slot_bytes), "pinned staging");
+      sl.host_bytes = slot_bytes;
+    }
     cuda_check(cudaEventCreate(&S->start), "event");
     cuda_check(cudaEventRecord(S->start, S->streams[0]), "event record");
     cuda_check(cudaEventSynchronize(S->start), "event sync");

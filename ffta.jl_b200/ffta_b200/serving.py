@@ -235,9 +235,12 @@ def run_one_by_one(trace, xs, ys, cache: PlanCache):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for r, x, y in zip(trace, xs, ys):
-        now = time.perf_counter() - t0
-        if now < r.arrival:
-            time.sleep(r.arrival - now)
+        while True:  # wait for the arrival (sleep long gaps, spin short ones)
+            gap = r.arrival - (time.perf_counter() - t0)
+            if gap <= 0:
+                break
+            if gap > 2e-4:
+                time.sleep(gap - 1e-4)
         _run_single(cache, r, x, y, stream)
         stream.synchronize()
         r.done = time.perf_counter() - t0
@@ -320,9 +323,11 @@ class Server:
                     done[tk[:c] - base] = tm[:c] * 1e-3
                 ndone += c
                 if cnt.value == 0 and nxt < n and ndone == nxt:
+                    # idle until the next arrival: sleep only for gaps well above
+                    # the OS timer's overshoot (tens of microseconds), else spin
                     dt = arrivals[nxt] - (time.perf_counter() - t0)
-                    if dt > 0:
-                        time.sleep(min(dt, 0.0005))
+                    if dt > 2e-4:
+                        time.sleep(min(dt - 1e-4, 0.0005))
         finally:
             st6 = (ctypes.c_int64 * 6)()
             _check(_lib.lib.fb_server_stats(h, st6, 6))
