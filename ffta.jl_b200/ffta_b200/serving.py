@@ -1,7 +1,7 @@
 """Continuous-batching transform server over the sm_100a library.
 
-FFTA.jl has no serving layer; this module is the request loop the north star
-asks for on top of the drop-in path.  Requests are (length n, element type,
+FFTA.jl has no serving layer; this module is a request loop on top of the
+drop-in path.  Requests are (length n, element type,
 direction, batch count, seed, arrival time).  The loop:
 
 * admits waiting requests in arrival order while their device bytes (input +
