@@ -417,7 +417,7 @@ template <class RL, int T> __host__ __device__ constexpr int max_values() {
 }
 template <typename R, class RL, int T, bool MID, bool PLAIN> struct TileBounds {
   static constexpr int min_blocks =
-      (sizeof(R) == 4 && !MID && T <= 512 && max_values<RL, T>() <= 18) ? 2 : 1;
+      (!MID && T <= 512 && max_values<RL, T>() <= (sizeof(R) == 4 ? 18 : 9)) ? 2 : 1;
 };
 // Whether a tile launch reserves shared memory for a staged twiddle slice:
 // only four-step passes whose slice follows the second batch level.
@@ -448,10 +448,10 @@ __device__ __forceinline__ const C* stage_twiddles(const LineArgs& a, const int6
 // threadIdx.x = g, threadIdx.y = u, so a warp spans 32/G butterflies of G
 // lines.  MID: forward program, multiply by a.mid, inverse program.
 template <typename R, class RL, int T, bool MID, bool PLAIN>
-// ComplexF32 blocks of up to 512 threads (except the Bluestein MID variant)
-// are held to 64 registers so two fit per SM -- measured faster than one block
-// with more registers, also where the full-I/O variant then spills a little --
-// unless a thread holds more than 18 values in some stage.
+// Blocks of up to 512 threads (except the Bluestein MID variant) are held to
+// 64 registers so two fit per SM -- measured faster than one block with more
+// registers, also where the full-I/O variant then spills a little -- unless a
+// thread holds more than 18 ComplexF32 or 9 ComplexF64 values in some stage.
 __global__ void __launch_bounds__(T > 512 ? T : 512, TileBounds<R, RL, T, MID, PLAIN>::min_blocks)
     fast_tile_kernel(const LineArgs a) {
   typedef cplx<R> C;
