@@ -1677,7 +1677,10 @@ struct fb_server_s {
   int device = 0;
   double budget = 100e9;
   std::vector<cudaStream_t> streams;
-  cudaStream_t serial = nullptr;  // multi-pass plans
+  // multi-pass plans: each plan keeps one of these streams (its scratch is
+  // then never used by two launches at once); different plans run side by side
+  std::vector<cudaStream_t> multi_streams;
+  std::map<const fb_plan_s*, int> multi_stream_of;
   cudaEvent_t start = nullptr;
   int next_stream = 0, next_slot = 0;
   std::map<std::tuple<int64_t, int, int>, std::unique_ptr<fb_plan_s>> templ;
@@ -1699,7 +1702,7 @@ struct fb_server_s {
       if (sl.host) cudaFreeHost(sl.host);
     }
     for (auto s : streams) cudaStreamDestroy(s);
-    if (serial) cudaStreamDestroy(serial);
+    for (auto s : multi_streams) cudaStreamDestroy(s);
     if (start) cudaEventDestroy(start);
   }
 };
@@ -1795,6 +1798,9 @@ static const SrvShape* srv_shape(fb_server_s* S, const fb_plan_s* T, int dtype) 
 // Requests one dispatch takes at most: a burst is cut into several launches
 // so building the next one's descriptors overlaps the GPU running this one.
 static const size_t kDispatchMax = 384;
+// Requests of at least this many elements are not packed into descriptor
+// launches of the generic kernel but run through their own cached plan.
+static const int64_t kPackedMaxElems = int64_t(1) << 18;
 
 static void srv_dispatch(fb_server_s* S) {
   std::vector<SrvReq> batch;
@@ -1819,10 +1825,16 @@ static void srv_dispatch(fb_server_s* S) {
   for (const SrvReq& r : batch) {
     if (!r.shape) {
       fb_plan_s* P = srv_multi(S, r.n, r.dtype, r.dir, r.batch);
-      execute_plan(P, r.in, r.out, S->serial);
+      auto ms = S->multi_stream_of.find(P);
+      if (ms == S->multi_stream_of.end())
+        ms = S->multi_stream_of
+                 .emplace(P, (int)(S->multi_stream_of.size() % S->multi_streams.size()))
+                 .first;
+      cudaStream_t mst = S->multi_streams[ms->second];
+      execute_plan(P, r.in, r.out, mst);
       SrvLaunch l;
       cuda_check(cudaEventCreateWithFlags(&l.ev, cudaEventDefault), "event");
-      cuda_check(cudaEventRecord(l.ev, S->serial), "event record");
+      cuda_check(cudaEventRecord(l.ev, mst), "event record");
       l.tickets.push_back(r.ticket);
       l.bytes = r.bytes;
       l.slot = -1;
@@ -1918,7 +1930,11 @@ int fb_server_create(fb_server* srv, double budget_bytes, int nstreams, uint32_t
       cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
       S->streams.push_back(st);
     }
-    cuda_check(cudaStreamCreateWithFlags(&S->serial, cudaStreamNonBlocking), "stream");
+    for (int i = 0; i < ns; ++i) {
+      cudaStream_t st;
+      cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+      S->multi_streams.push_back(st);
+    }
     // descriptor slots sized for the largest dispatch up front: growing one
     // later frees device memory (which synchronises the device) and
     // allocates pinned memory in the middle of serving
@@ -1948,7 +1964,10 @@ int fb_server_submit(fb_server srv, int64_t n, int dtype, int dir, int64_t batch
     // plans are made at submission (tables resident); bytes = data + scratch
     fb_plan_s* T = srv_template(srv, n, dtype, dir);
     double bytes = 2.0 * (double)n * (double)batch * elem_bytes(dtype);
-    const SrvShape* shape = srv_single_pass(T) ? srv_shape(srv, T, dtype) : nullptr;
+    // large single-pass requests run their own plan (specialised kernels) on
+    // a plan stream; small ones are packed into descriptor launches
+    const bool packed = srv_single_pass(T) && n * batch < kPackedMaxElems;
+    const SrvShape* shape = packed ? srv_shape(srv, T, dtype) : nullptr;
     if (!shape) bytes += (double)plan_scratch_bytes(srv_multi(srv, n, dtype, dir, batch));
     SrvReq r{srv->next_ticket++, n, batch, dtype, dir, in, out, bytes, shape};
     srv->pending.push_back(r);

@@ -9,10 +9,11 @@ direction, batch count, seed, arrival time).  The loop:
   a request's bytes when it completes;
 * keeps plans (twiddle/chirp tables, scratch) resident, keyed by
   (n, type, direction) -- and the batch for multi-pass lengths;
-* packs every admitted single-pass request -- any mix of lengths, types and
-  directions -- into one work-descriptor launch per kernel variant (each
-  block looks up its request's descriptor); multi-pass lengths run their
-  cached plans on a dedicated stream;
+* packs every admitted small single-pass request -- any mix of lengths,
+  types and directions -- into one work-descriptor launch per kernel variant
+  (each block looks up its request's descriptor); multi-pass lengths and
+  large requests (2^18 elements or more) run their cached plans, each plan on
+  a stream of its own so different plans overlap;
 * rotates launches over several CUDA streams and dispatches whatever arrived
   while earlier launches run, as soon as a stream is free (continuous
   batching); completions are timed with CUDA events on the device clock.
