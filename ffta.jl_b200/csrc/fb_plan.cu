@@ -1629,13 +1629,14 @@ extern "C" int fb_plan_create_real(fb_plan* plan, int dtype, int dir, int rank,
 // Continuous batching over work-descriptor launches.  Requests (n, type,
 // direction, batch, device in/out) wait in arrival order; dispatch() admits
 // them while their bytes fit the budget and
-//  * packs every admitted request whose length runs in one pass into
-//    work-descriptor launches of the generic kernel (one per kernel variant,
-//    block size and shared-memory class) -- requests of different lengths and
-//    directions share a launch;
-//  * runs multi-pass lengths (four-step, three-pass Bluestein) with a cached
-//    per-(n, type, direction, batch) plan on one dedicated stream, so that
-//    their plan-owned scratch is never used by two requests at once.
+//  * packs every admitted request whose length runs in one pass and that has
+//    fewer than kPackedMaxElems elements into work-descriptor launches of the
+//    generic kernel (one per kernel variant, block size and shared-memory
+//    class) -- requests of different lengths and directions share a launch;
+//  * runs multi-pass lengths (four-step, three-pass Bluestein) and large
+//    requests with a cached per-(n, type, direction, batch) plan, each plan
+//    bound to one plan stream, so that a plan's scratch is never used by two
+//    requests at once while different plans overlap.
 // Launches rotate over the server's streams; poll() retires completed ones
 // and dispatches what has arrived since, so new requests join as earlier
 // ones finish.

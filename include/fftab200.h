@@ -145,8 +145,9 @@ int fb_execute_grouped(fb_plan plan, int64_t count, const void* const* ins, void
  * requests in arrival order while their device bytes (input + output + any
  * multi-pass scratch) fit `budget_bytes`, packs all admitted single-pass
  * requests -- any mix of lengths, types and directions -- into one kernel
- * launch per kernel variant, runs multi-pass lengths with cached plans on a
- * dedicated stream, and rotates launches over `nstreams` CUDA streams. */
+ * launch per kernel variant, runs multi-pass lengths and large requests
+ * (2^18 elements or more) with cached plans, each plan on one of `nstreams`
+ * plan streams, and rotates launches over `nstreams` CUDA streams. */
 typedef struct fb_server_s* fb_server;
 int fb_server_create(fb_server* srv, double budget_bytes, int nstreams, uint32_t flags);
 /* Queue `batch` contiguous transforms of length n (device pointers; the
