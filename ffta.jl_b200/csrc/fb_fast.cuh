@@ -65,6 +65,17 @@ __host__ __device__ constexpr int lpad_of(int L) {
                                                : (L - 1) + ((L - 1) >> 4) + 2;
 }
 
+// Shared-memory slot of element e of a line.  Power-of-two strides would hit
+// the same banks, so even lengths skip one slot every 16 (padi); odd lengths
+// (powers of three and 5-smooth odd lengths) have only odd strides, which
+// spread over the banks by themselves, and are stored flat.
+template <class RL> __device__ __forceinline__ int pidx(int e) {
+  if constexpr (prog_len<RL>() % 2 == 1)
+    return e;
+  else
+    return padi(e);
+}
+
 // ---------------------------------------------------------------- I/O
 // A stage's input or output is shared memory (SmemIO) or a functor that
 // loads element i of the line / stores element i of the line.
@@ -228,7 +239,7 @@ __device__ __forceinline__ void fast_stage(cplx<R>* buf, const In& in, const Out
         if constexpr (GIN)
           v[q][r] = in.raw(j + r * nb);
         else
-          v[q][r] = buf[padi(j + r * nb)];
+          v[q][r] = buf[pidx<RL>(j + r * nb)];
       }
     }
   }
@@ -265,7 +276,7 @@ __device__ __forceinline__ void fast_stage(cplx<R>* buf, const In& in, const Out
         if constexpr (GOUT)
           out(base + r * Ns, v[q][r]);
         else
-          buf[padi(base + r * Ns)] = v[q][r];
+          buf[pidx<RL>(base + r * Ns)] = v[q][r];
       }
     }
   }
@@ -506,7 +517,7 @@ __global__ void __launch_bounds__(T > 512 ? T : 512, TileBounds<R, RL, T, MID, P
       fast_prog<R, -1, RL, T>(buf, in, SmemIO{}, tw, pcs, u);
       const C* __restrict__ mid = (const C*)a.mid;
       for (int k = u; k < L; k += T)
-        buf[padi(k)] = cmul<R>(buf[padi(k)], __ldg(mid + l0 * a.mid_ls + (int64_t)k * a.mid_es));
+        buf[pidx<RL>(k)] = cmul<R>(buf[pidx<RL>(k)], __ldg(mid + l0 * a.mid_ls + (int64_t)k * a.mid_es));
       __syncthreads();
       fast_prog<R, 1, RL, T>(buf, SmemIO{}, out, tw, pcs, u);
     } else {
