@@ -349,10 +349,18 @@ static bool make_line(int64_t n, int64_t cutoff, int dtype, LineX* x) {
   return make_blue1(n, dtype, x);
 }
 
-static double line_cost(const LineX& x) {
+// Relative cost of one line: work ~ L (log2 L + 4).  With `weighted` (splits
+// of lengths that are not powers of two) the work is scaled by how close the
+// length's kernels come to copy bandwidth: powers of two from 256 (radix-16
+// programs) 1.0, lines shorter than 16 2.0, others 1.25 -- measured on the
+// four-step splits of 27648: 1024 x 27 in 0.182 ms, 144 x 192 in 0.226 ms.
+static double line_cost(const LineX& x, bool weighted = false) {
   const double L = x.L;
   const double c = L * (std::log2(std::max(2.0, L)) + 4.0);
-  return x.kind == 0 ? c : 2.0 * c + 2.0 * L;
+  double eff = 1.0;
+  if (weighted)
+    eff = (x.L >= 256 && (x.L & (x.L - 1)) == 0) ? 1.0 : (x.L < 16 ? 2.0 : 1.25);
+  return x.kind == 0 ? c * eff : 2.0 * c + 2.0 * L;
 }
 
 // ------------------------------------------------------------------ plan
@@ -1103,9 +1111,12 @@ static Axis plan_axis(fb_plan_s* P, int64_t n, int64_t is, int64_t os, std::vect
       LineX xa, xb;
       if (!make_line(a, P->cutoff, P->dtype, &xa) || !make_line(b, P->cutoff, P->dtype, &xb)) continue;
       if (prefer_split && (xa.kind != 0 || xb.kind != 0)) continue;
-      double c = line_cost(xa) * (double)b + line_cost(xb) * (double)a;
-      // prefer balanced direct splits on ties
+      const bool weighted = (n & (n - 1)) != 0;
+      double c = line_cost(xa, weighted) * (double)b + line_cost(xb, weighted) * (double)a;
+      // prefer balanced direct splits on ties, and the power-of-two factor
+      // as the first pass (the strided columns)
       c *= 1.0 + 1e-9 * std::fabs(std::log((double)a) - std::log((double)b));
+      if ((a & (a - 1)) == 0 && (b & (b - 1)) != 0) c *= 1.0 - 1e-6;
       if (c < best) {
         best = c;
         bN1 = a;
