@@ -388,6 +388,7 @@ def main():
                                      "one_launch_per_request":
                                          sat["one_launch_per_request"]["p99_ms"]},
                 **res}
+        serving_out["recurring_multipass_graphs"] = S.compare_graphs()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -1705,9 +1705,29 @@ struct fb_server_s {
   std::deque<std::pair<int64_t, double>> done;
   // per template plan: its descriptor launch shape, computed once
   std::map<const fb_plan_s*, fb::SrvShape> shapes;
+  // CUDA graphs of multi-pass plans keyed by (plan, input, output): a request
+  // shape that recurs on the same buffers is captured on its second
+  // occurrence and replayed as one graph launch from then on
+  typedef std::tuple<const fb_plan_s*, const void*, void*> GraphKey;
+  struct Graph {
+    cudaGraphExec_t exec;
+    cudaStream_t st;
+    int64_t used;
+  };
+  bool graphs = true;
+  std::map<GraphKey, int> seen;
+  std::map<GraphKey, Graph> graph_of;
+  // released graphs, destroyed once the event after their last launch is done
+  std::vector<std::pair<cudaEvent_t, cudaGraphExec_t>> graph_retiring;
+  int64_t graph_clock = 0, st_graph_launches = 0, st_graph_captures = 0;
   int64_t st_launches = 0, st_desc_launches = 0, st_requests = 0, st_max_queue = 0;
   double st_max_admitted = 0;
   ~fb_server_s() {
+    for (auto& g : graph_of) cudaGraphExecDestroy(g.second.exec);
+    for (auto& g : graph_retiring) {
+      cudaEventDestroy(g.first);
+      cudaGraphExecDestroy(g.second);
+    }
     for (auto& l : inflight) cudaEventDestroy(l.ev);
     for (auto& sl : slots) {
       if (sl.last) cudaEventDestroy(sl.last);
@@ -1758,7 +1778,82 @@ static size_t plan_scratch_bytes(const fb_plan_s* P) {
   return b;
 }
 
+// Graphs kept per server; the least recently used one is released first.
+static const size_t kGraphCacheMax = 1024;
+
+// Destroy the released graphs whose last launch has finished.
+static void srv_sweep_graphs(fb_server_s* S) {
+  auto& v = S->graph_retiring;
+  for (size_t i = 0; i < v.size();) {
+    const cudaError_t q = cudaEventQuery(v[i].first);
+    if (q == cudaErrorNotReady) {
+      ++i;
+      continue;
+    }
+    cuda_check(q, "graph release");
+    cudaEventDestroy(v[i].first);
+    cudaGraphExecDestroy(v[i].second);
+    v[i] = v.back();
+    v.pop_back();
+  }
+}
+
+// Run multi-pass plan P on (in, out) in stream st: plain launches the first
+// time a (plan, in, out) key is seen, a captured graph from the second time.
+// Capture only records the launches (relaxed mode, nothing runs), so the
+// graph's kernels and arguments are exactly those of execute_plan.
+static void srv_run_plan(fb_server_s* S, fb_plan_s* P, const void* in, void* out,
+                         cudaStream_t st) {
+  if (!S->graphs) {
+    execute_plan(P, in, out, st);
+    return;
+  }
+  const fb_server_s::GraphKey key(P, in, out);
+  auto g = S->graph_of.find(key);
+  if (g == S->graph_of.end()) {
+    if (S->seen.size() >= 16 * kGraphCacheMax) S->seen.clear();
+    if (++S->seen[key] < 2) {
+      execute_plan(P, in, out, st);
+      return;
+    }
+    if (S->graph_of.size() >= kGraphCacheMax) {
+      auto lru = S->graph_of.begin();
+      for (auto it = S->graph_of.begin(); it != S->graph_of.end(); ++it)
+        if (it->second.used < lru->second.used) lru = it;
+      // released after its last launch: an event behind it on its stream
+      cudaEvent_t ev = nullptr;
+      cuda_check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+      cuda_check(cudaEventRecord(ev, lru->second.st), "event record");
+      S->graph_retiring.push_back({ev, lru->second.exec});
+      S->graph_of.erase(lru);
+      srv_sweep_graphs(S);
+    }
+    cudaGraph_t graph = nullptr;
+    cuda_check(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed), "graph capture");
+    try {
+      execute_plan(P, in, out, st);
+    } catch (...) {
+      cudaStreamEndCapture(st, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      throw;
+    }
+    cuda_check(cudaStreamEndCapture(st, &graph), "graph capture");
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    cuda_check(e, "graph instantiate");
+    g = S->graph_of.emplace(key, fb_server_s::Graph{exec, st, 0}).first;
+    S->seen.erase(key);
+    S->st_graph_captures += 1;
+  }
+  g->second.used = ++S->graph_clock;
+  g->second.st = st;
+  cuda_check(cudaGraphLaunch(g->second.exec, st), "graph launch");
+  S->st_graph_launches += 1;
+}
+
 static void srv_retire(fb_server_s* S, bool block) {
+  if (!S->graph_retiring.empty()) srv_sweep_graphs(S);
   while (!S->inflight.empty()) {
     bool done_any = false;
     for (auto it = S->inflight.begin(); it != S->inflight.end();) {
@@ -1843,7 +1938,7 @@ static void srv_dispatch(fb_server_s* S) {
                  .emplace(P, (int)(S->multi_stream_of.size() % S->multi_streams.size()))
                  .first;
       cudaStream_t mst = S->multi_streams[ms->second];
-      execute_plan(P, r.in, r.out, mst);
+      srv_run_plan(S, P, r.in, r.out, mst);
       SrvLaunch l;
       cuda_check(cudaEventCreateWithFlags(&l.ev, cudaEventDefault), "event");
       cuda_check(cudaEventRecord(l.ev, mst), "event record");
@@ -1924,7 +2019,6 @@ static void srv_dispatch(fb_server_s* S) {
 extern "C" {
 
 int fb_server_create(fb_server* srv, double budget_bytes, int nstreams, uint32_t flags) {
-  (void)flags;
   return guard([&] {
     if (!srv) fail(FB_ERR_ARGUMENT, "null argument");
     *srv = nullptr;
@@ -1936,6 +2030,7 @@ int fb_server_create(fb_server* srv, double budget_bytes, int nstreams, uint32_t
     std::unique_ptr<fb_server_s> S(new fb_server_s());
     cuda_check(cudaGetDevice(&S->device), "cudaGetDevice");
     S->budget = budget_bytes > 0 ? budget_bytes : 100e9;
+    S->graphs = !(flags & FB_SERVER_NO_GRAPHS);
     const int ns = std::max(1, std::min(nstreams, 16));
     for (int i = 0; i < ns; ++i) {
       cudaStream_t st;
@@ -2031,10 +2126,11 @@ int fb_server_wait(fb_server srv) {
 int fb_server_stats(fb_server srv, int64_t* out, int nout) {
   return guard([&] {
     if (!srv || !out) fail(FB_ERR_ARGUMENT, "null argument");
-    const int64_t v[6] = {srv->st_requests, srv->st_launches, srv->st_desc_launches,
+    const int64_t v[8] = {srv->st_requests, srv->st_launches, srv->st_desc_launches,
                           srv->st_max_queue, (int64_t)srv->st_max_admitted,
-                          (int64_t)(srv->templ.size() + srv->multi.size())};
-    for (int i = 0; i < nout && i < 6; ++i) out[i] = v[i];
+                          (int64_t)(srv->templ.size() + srv->multi.size()),
+                          srv->st_graph_launches, srv->st_graph_captures};
+    for (int i = 0; i < nout && i < 8; ++i) out[i] = v[i];
   });
 }
 

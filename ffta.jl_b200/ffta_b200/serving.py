@@ -38,7 +38,7 @@ import time
 
 import numpy as np
 
-from . import _lib, _check, plan_fft, plan_bfft
+from . import _lib, _check, plan_fft, plan_bfft, FB_SERVER_NO_GRAPHS
 
 ELEM = {"c64": 8, "c128": 16}
 
@@ -253,15 +253,25 @@ class Server:
     request when it arrives and polls for completions.  Admission, packing
     into work-descriptor launches and stream rotation happen in the library.
     Completion times come from CUDA events on the device clock, counted from
-    the server's creation (the run's time origin)."""
+    the server's creation (the run's time origin).  With `graphs`, a
+    multi-pass request that recurs on the same buffers is replayed from a
+    CUDA graph captured on its second occurrence."""
 
     KIND = {"c64": _lib.FB_C32, "c128": _lib.FB_C64}
+    NSTATS = 8
 
-    def __init__(self, budget_bytes: float = 100e9, nstreams: int = 4):
+    def __init__(self, budget_bytes: float = 100e9, nstreams: int = 4, graphs: bool = True):
         self.budget = budget_bytes
         self.nstreams = nstreams
         self.h = ctypes.c_void_p()
-        _check(_lib.lib.fb_server_create(ctypes.byref(self.h), float(budget_bytes), nstreams, 0))
+        flags = 0 if graphs else FB_SERVER_NO_GRAPHS
+        _check(_lib.lib.fb_server_create(ctypes.byref(self.h), float(budget_bytes), nstreams,
+                                         flags))
+
+    def stats(self):
+        st = (ctypes.c_int64 * self.NSTATS)()
+        _check(_lib.lib.fb_server_stats(self.h, st, self.NSTATS))
+        return list(st)
 
     def __del__(self):
         try:
@@ -275,8 +285,7 @@ class Server:
         import torch
         torch.cuda.synchronize()
         h = self.h
-        st0 = (ctypes.c_int64 * 6)()
-        _check(_lib.lib.fb_server_stats(h, st0, 6))
+        st0 = self.stats()
         n = len(trace)
         # request fields as arrays, so that everything that has arrived is
         # submitted with one call
@@ -330,14 +339,14 @@ class Server:
                     if dt > 2e-4:
                         time.sleep(min(dt - 1e-4, 0.0005))
         finally:
-            st6 = (ctypes.c_int64 * 6)()
-            _check(_lib.lib.fb_server_stats(h, st6, 6))
+            st1 = self.stats()
         for r, d in zip(trace, done):
             r.done = float(d)
         out = _stats(trace, time.perf_counter() - t0, "continuous_batching")
-        out.update({"launches": st6[1] - st0[1], "descriptor_launches": st6[2] - st0[2],
-                    "max_queue": st6[3], "max_admitted_GB": st6[4] / 1e9,
-                    "resident_plans": st6[5], "streams": self.nstreams})
+        out.update({"launches": st1[1] - st0[1], "descriptor_launches": st1[2] - st0[2],
+                    "max_queue": st1[3], "max_admitted_GB": st1[4] / 1e9,
+                    "resident_plans": st1[5], "graph_launches": st1[6] - st0[6],
+                    "graph_captures": st1[7] - st0[7], "streams": self.nstreams})
         return out
 
 
@@ -355,6 +364,41 @@ def check_mix_equals_alone(trace, xs, ys_mix, cache: PlanCache):
 
 
 # ------------------------------------------------------------ benchmark
+def compare_graphs(count=600, seed=13, nstreams=4, repeats=5):
+    """Recurring small multi-pass requests (four-step and three-pass Bluestein
+    lengths, batch 1..4, below the packing limit, so each runs its cached
+    plan: 2-3 kernels), all queued at once, served again and again on the
+    same buffers by a server that replays CUDA graphs and by one that
+    launches the plans' kernels each time.  Two warm-up runs each (plans,
+    then graphs), then the median of `repeats` runs.  Results of the two must
+    be equal bit for bit."""
+    import torch
+    rng = np.random.default_rng(seed)
+    lengths = [20000, 32768, 40000, 65536, 65537, 100003, 24576, 50000]
+    reqs = [Request(i, int(rng.choice(lengths)), "c128" if rng.random() < 0.2 else "c64",
+                    -1 if rng.random() < 0.5 else 1, int(rng.integers(1, 5)),
+                    int(rng.integers(0, 2 ** 31)), 0.0) for i in range(count)]
+    xs = make_inputs(reqs, "cuda")
+    out = {}
+    ys_of = {}
+    for label, graphs in (("graphs", True), ("no_graphs", False)):
+        ys = [torch.empty_like(x) for x in xs]
+        srv = Server(100e9, nstreams, graphs=graphs)
+        for _ in range(2):
+            srv.run([dataclasses.replace(r) for r in reqs], xs, ys)
+        runs = [srv.run([dataclasses.replace(r) for r in reqs], xs, ys) for _ in range(repeats)]
+        runs.sort(key=lambda st: st["throughput_req_s"])
+        out[label] = runs[len(runs) // 2]
+        ys_of[label] = ys
+        del srv
+    diff = max((a - b).abs().max().item() for a, b in zip(ys_of["graphs"], ys_of["no_graphs"]))
+    out["throughput_ratio"] = (out["graphs"]["throughput_req_s"] /
+                               out["no_graphs"]["throughput_req_s"])
+    out["graphs_vs_launches_max_abs_diff"] = diff
+    out["notes"] = {"requests": count, "lengths": lengths, "batch": "1..4", "repeats": repeats}
+    return out
+
+
 def compare(count=400, rates=(2000.0,), seed=11, n_max=2 ** 20, batch_max=512,
             max_elems=1 << 22, budget_bytes=100e9, nstreams=4):
     """Serve one trace with both paths at each arrival rate of a sweep.
@@ -376,7 +420,10 @@ def compare(count=400, rates=(2000.0,), seed=11, n_max=2 ** 20, batch_max=512,
     xs = make_inputs(base, "cuda")
     ys = [torch.empty_like(x) for x in xs]
     srv = Server(budget_bytes, nstreams)
-    srv.run([dataclasses.replace(r, arrival=0.0) for r in base], xs, ys)  # resident plans
+    # two warm-up passes: resident plans, then graphs of the multi-pass
+    # requests (each runs again on the same buffers in every sweep point)
+    for _ in range(2):
+        srv.run([dataclasses.replace(r, arrival=0.0) for r in base], xs, ys)
     run_one_by_one([dataclasses.replace(r, arrival=0.0) for r in base[:8]], xs[:8], ys[:8], cache)
     worst = check_mix_equals_alone(base[:50], xs[:50], ys[:50], cache)
     sweep = []

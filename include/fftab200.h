@@ -147,7 +147,13 @@ int fb_execute_grouped(fb_plan plan, int64_t count, const void* const* ins, void
  * requests -- any mix of lengths, types and directions -- into one kernel
  * launch per kernel variant, runs multi-pass lengths and large requests
  * (2^18 elements or more) with cached plans, each plan on one of `nstreams`
- * plan streams, and rotates launches over `nstreams` CUDA streams. */
+ * plan streams, and rotates launches over `nstreams` CUDA streams.  A
+ * multi-pass request whose (length, type, direction, batch, input, output)
+ * recurs is captured into a CUDA graph on its second occurrence and replayed
+ * as one graph launch afterwards (at most 1024 graphs per server, least
+ * recently used released first); FB_SERVER_NO_GRAPHS in `flags` turns this
+ * off. */
+enum { FB_SERVER_NO_GRAPHS = 1u };
 typedef struct fb_server_s* fb_server;
 int fb_server_create(fb_server* srv, double budget_bytes, int nstreams, uint32_t flags);
 /* Queue `batch` contiguous transforms of length n (device pointers; the
@@ -166,8 +172,9 @@ int fb_server_submit_many(fb_server srv, int64_t count, const int64_t* n, const 
 int fb_server_poll(fb_server srv, int64_t max, int64_t* tickets, double* done_ms, int64_t* count);
 /* Dispatch and wait until every submitted request has completed. */
 int fb_server_wait(fb_server srv);
-/* out[0..5]: requests, launches, descriptor launches, max queue depth, max
- * admitted bytes, resident plans. */
+/* out[0..7]: requests, launches, descriptor launches, max queue depth, max
+ * admitted bytes, resident plans, graph launches, graph captures (the first
+ * `nout` of them). */
 int fb_server_stats(fb_server srv, int64_t* out, int nout);
 /* Restart the clock of fb_server_poll's completion times (waits until the
  * server's first stream is idle). */

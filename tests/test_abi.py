@@ -73,3 +73,13 @@ def test_status_codes_before_device():
     assert _lib.lib.fb_plan_create_nd(ctypes.byref(h), 0, -1, 2, dims, st, st, 2, reg2, 73, 0) == \
         _lib.FB_ERR_DIMENSION_MISMATCH
     assert _lib.last_error() == "Region is invalid."
+
+
+def test_header_flags_match_python_constants():
+    import re
+    import ffta_b200 as F
+    text = open(HEADER).read()
+    defs = dict(re.findall(r"\b(FB_(?:FLAG|SERVER)_\w+)\s*=\s*(\d+)u?", text))
+    assert "FB_SERVER_NO_GRAPHS" in defs and "FB_FLAG_TENSOR_STAGE" in defs
+    for name, val in defs.items():
+        assert getattr(F, name) == int(val), name

@@ -64,3 +64,59 @@ def test_one_launch_for_mixed_requests():
     for r, x, y in zip(reqs, xs, ys):
         f = F.fft if r.dir < 0 else F.bfft
         assert torch.equal(y, f(x.T, 1).T), r
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("graphs", [True, False])
+def test_recurring_multipass_requests_replay_graphs(graphs):
+    """Multi-pass requests (three-pass Bluestein, four-step) and large
+    single-pass ones run through cached plans; when the same request recurs on
+    the same buffers it is captured into a CUDA graph on its second occurrence
+    and replayed from the third on.  Replayed results equal the plans' own
+    launches bit for bit."""
+    import torch
+    import ffta_b200 as F
+    spec = [(65537, "c64", -1, 1), (32768, "c64", 1, 2), (19683, "c128", 1, 1),
+            (4096, "c64", -1, 64), (1000, "c64", 1, 3)]
+    reqs = [serving.Request(i, n, k, d, b, i, 0.0) for i, (n, k, d, b) in enumerate(spec)]
+    xs = serving.make_inputs(reqs, "cuda")
+    ys = [torch.empty_like(x) for x in xs]
+    srv = serving.Server(nstreams=2, graphs=graphs)
+    plan_runs = 4  # every request but the packed 1000 x 3
+    st = [srv.run(reqs, xs, ys)]
+    for _ in range(2):
+        for y in ys:
+            y.fill_(float("nan"))
+        st.append(srv.run(reqs, xs, ys))
+    if graphs:
+        assert [s["graph_captures"] for s in st] == [0, plan_runs, 0]
+        assert [s["graph_launches"] for s in st] == [0, plan_runs, plan_runs]
+    else:
+        assert all(s["graph_captures"] == 0 and s["graph_launches"] == 0 for s in st)
+    for r, x, y in zip(reqs, xs, ys):
+        f = F.fft if r.dir < 0 else F.bfft
+        assert torch.equal(y, f(x.T, 1).T), r
+
+
+@pytest.mark.gpu
+def test_graph_cache_releases_least_recently_used():
+    """More recurring (plan, buffers) keys than the server keeps graphs for
+    (1024): the least recently used graphs are released while later launches
+    run, and every result still equals the plan's own launch."""
+    import torch
+    import ffta_b200 as F
+    count = 1100
+    reqs = [serving.Request(i, 20000, "c64", -1 if i % 2 else 1, 1, i, 0.0) for i in range(count)]
+    base = torch.randn(count, 20000, dtype=torch.complex64, device="cuda")
+    xs = [base[i:i + 1] for i in range(count)]
+    ys = [torch.empty_like(x) for x in xs]
+    srv = serving.Server(nstreams=2)
+    st = [srv.run(reqs, xs, ys) for _ in range(3)]
+    # run 2 captures every key (evicting the first 76 again); run 3 replays
+    # the 1024 kept and sees the evicted ones for the first time since
+    assert [s["graph_captures"] for s in st] == [0, count, 0]
+    assert [s["graph_launches"] for s in st] == [0, count, 1024]
+    fwd = F.fft(base.T, 1).T
+    bwd = F.bfft(base.T, 1).T
+    for i, y in enumerate(ys):
+        assert torch.equal(y[0], (fwd if i % 2 else bwd)[i]), i
