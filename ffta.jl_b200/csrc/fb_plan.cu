@@ -454,6 +454,15 @@ namespace fb {
 static int pick_G(const fb_plan_s* P, int L, int T, int Lpad, bool elem_major, int64_t nlines);
 static void apply_tuning(fb_plan_s* P);
 
+// Lines per block of the tile kernel: by its threads (up to 512 per block),
+// and by shared memory -- 100 KB for ComplexF32; ComplexF64 tiles run faster
+// at about 40 KB (more resident blocks per SM, measured).
+static int tile_thread_cap(const FastFn* ff) { return std::max(1, std::max(512, ff->T) / ff->T); }
+static int tile_smem_cap(const FastFn* ff, int es) {
+  const size_t budget = es == 8 ? 100 * 1024 : 40 * 1024;
+  return (int)std::max<size_t>(1, budget / ((size_t)(ff->lpad + 15) * es + 32));
+}
+
 // Switch a generic pass to the compile-time tile kernel of its length when
 // one is compiled (same arithmetic, direct HBM I/O, lines fastest across a
 // warp).  Bluestein passes need the forward-then-inverse order it implements.
@@ -464,11 +473,7 @@ static void use_tile(const fb_plan_s* P, Pass& p, const std::vector<int>& radice
   if (p.a.mid && (p.a.dir1 > 0 || p.a.dir2 < 0)) return;
   const int es = elem_bytes(P->dtype);
   const int T = ff->T;
-  const int thr_cap = std::max(1, std::max(512, T) / T);
-  // shared memory per block: 100 KB for ComplexF32; ComplexF64 tiles run
-  // faster at about 40 KB (more resident blocks per SM, measured)
-  const size_t budget = es == 8 ? 100 * 1024 : 40 * 1024;
-  const int smem_cap = (int)std::max<size_t>(1, budget / ((size_t)(ff->lpad + 15) * es + 32));
+  const int thr_cap = tile_thread_cap(ff), smem_cap = tile_smem_cap(ff, es);
   const bool em = p.a.ld.mode == 1 || p.a.st.mode == 1;
   // strided tiles: as many neighbouring lines as the block allows (longer
   // contiguous runs per DRAM page); contiguous lines: 128-thread blocks
@@ -1068,15 +1073,25 @@ static Axis plan_axis(fb_plan_s* P, int64_t n, int64_t is, int64_t os, std::vect
   bd = normalize_batch(bd);
   LineX x;
   // A strided axis whose neighbouring lines are neighbours in memory: one
-  // pass holds only as many lines as fit shared memory, so a long line gives
-  // short contiguous runs.  Below 128-byte runs prefer a four-step split whose
+  // pass holds only as many lines as fit a block, so a long line gives short
+  // contiguous runs per row.  The tile kernel of a compiled length keeps one
+  // pass while its block covers a whole 32-byte sector per row (measured: one
+  // pass is 10-34 % faster than the split there, and slower below); other
+  // lengths want 128-byte runs.  Shorter runs prefer a four-step split whose
   // passes hold many lines (FOURT order, see plan_four_axis).
   const bool strided = is != 1 && !bd.empty() && bd[0].is == 1 && bd[0].os == 1 && bd[0].n > 1;
   bool prefer_split = false;
   if (strided && make_direct(n, P->cutoff, P->dtype, &x)) {
     const int es = elem_bytes(P->dtype);
-    const int lines = std::max(1, (int)((100 * 1024) / ((size_t)lpad_for(x.L) * es)));
-    prefer_split = (int64_t)std::min(lines, 16) * es < 128 && !(P->flags & FB_FLAG_SAME_SCHEDULE_STRIDED);
+    const FastFn* ff = (P->flags & FB_FLAG_GENERIC_ONLY) ? nullptr
+                                                          : find_fast(P->dtype, x.L, x.radices);
+    int lines = std::min(16, std::max(1, (int)((100 * 1024) / ((size_t)lpad_for(x.L) * es))));
+    int need = 128;
+    if (ff && (int)ff->lpad == lpad_for(x.L) && x.kind == 0) {
+      lines = std::min(tile_thread_cap(ff), tile_smem_cap(ff, es));
+      need = 32;
+    }
+    prefer_split = (int64_t)lines * es < need && !(P->flags & FB_FLAG_SAME_SCHEDULE_STRIDED);
   }
   if (!prefer_split && make_direct(n, P->cutoff, P->dtype, &x))
     return plan_direct_axis(P, n, x, is, os, bd, src, dst);
