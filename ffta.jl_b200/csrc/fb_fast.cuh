@@ -85,11 +85,23 @@ struct SmemIO {};
 // fin(i, v) applies what depends on the element (tables, twiddles).  A stage
 // issues all of its raw loads before any fin, so every data load is in flight
 // before the table loads take registers.
+//
+// Cache hints.  A pass reads each input element once, so data loads are
+// streaming (evict-first in L2): the misses of a pass then displace each
+// other rather than the lines of its input that are still resident (the
+// previous pass's output).  Stores are evict-first only in a plan's last pass
+// (`cs`); an earlier pass leaves its output in L2 for the next one.
+template <typename R> __device__ __forceinline__ void store(cplx<R>* p, cplx<R> v, bool cs) {
+  if (cs)
+    __stcs(p, v);
+  else
+    *p = v;
+}
 template <typename R> struct DirectIn {
   const cplx<R>* __restrict__ g;
   bool ok;
   __device__ __forceinline__ cplx<R> raw(int i) const {
-    return ok ? g[i] : Sc<R>::mk(R(0), R(0));
+    return ok ? __ldcs(g + i) : Sc<R>::mk(R(0), R(0));
   }
   __device__ __forceinline__ cplx<R> fin(int, cplx<R> v) const { return v; }
 };
@@ -97,8 +109,9 @@ template <typename R> struct DirectOut {
   cplx<R>* __restrict__ g;
   bool ok;
   R scale;
+  bool cs;
   __device__ __forceinline__ void operator()(int i, cplx<R> v) const {
-    if (ok) g[i] = scale == R(1) ? v : cscale<R>(v, scale);
+    if (ok) store<R>(g + i, scale == R(1) ? v : cscale<R>(v, scale), cs);
   }
 };
 
@@ -116,7 +129,7 @@ template <typename R> struct TileIn {
   __device__ __forceinline__ cplx<R> raw(int i) const {
     const int64_t vi = (int64_t)i * ves + voff;
     if (!ok || vi >= vn) return Sc<R>::mk(R(0), R(0));
-    return base[(int64_t)i * es];
+    return __ldcs(base + (int64_t)i * es);
   }
   __device__ __forceinline__ cplx<R> fin(int i, cplx<R> v) const {
     const int64_t vi = (int64_t)i * ves + voff;
@@ -144,6 +157,7 @@ template <typename R> struct TileOut {
   bool ok;
   const cplx<R>* __restrict__ tab;  // full twiddle table (precedence over hi/lo)
   int64_t tab_es, tab_off;
+  bool cs;
   __device__ __forceinline__ void operator()(int i, cplx<R> v) const {
     const int64_t vi = (int64_t)i * ves + voff;
     if (!ok || vi >= vn) return;
@@ -158,7 +172,7 @@ template <typename R> struct TileOut {
       v = tw_dir < 0 ? cmul<R>(v, w) : cmulc<R>(v, w);
     }
     if (scale != R(1)) v = cscale<R>(v, scale);
-    base[(int64_t)i * es] = v;
+    store<R>(base + (int64_t)i * es, v, cs);
   }
 };
 
@@ -172,7 +186,7 @@ template <typename R> struct PlainIn {
   int es;
   const cplx<R>* tab;  // twiddle on load (LineArgs::tw_on_load)
   int tab_es, tab_off, tw_dir;
-  __device__ __forceinline__ cplx<R> raw(int i) const { return base[(int64_t)(i * es)]; }
+  __device__ __forceinline__ cplx<R> raw(int i) const { return __ldcs(base + (int64_t)(i * es)); }
   __device__ __forceinline__ cplx<R> fin(int i, cplx<R> v) const {
     if (tab) {
       const cplx<R> w = tab[i * tab_es + tab_off];
@@ -188,13 +202,14 @@ template <typename R> struct PlainOut {
   int tab_es, tab_off, tw_dir;
   R scale;
   bool ok;
+  bool cs;
   __device__ __forceinline__ void operator()(int i, cplx<R> v) const {
     if (tab) {
       const cplx<R> w = tab[i * tab_es + tab_off];
       v = tw_dir < 0 ? cmul<R>(v, w) : cmulc<R>(v, w);
     }
     if (scale != R(1)) v = cscale<R>(v, scale);
-    if (ok) base[(int64_t)(i * es)] = v;
+    if (ok) store<R>(base + (int64_t)(i * es), v, cs);
   }
 };
 
@@ -328,7 +343,7 @@ __global__ void __launch_bounds__(DirectBounds<R, T>::threads, DirectBounds<R, T
     gout = (C*)a.outs[lo] + k * a.odist;
   }
   const DirectIn<R> in{gin, ok};
-  const DirectOut<R> out{gout, ok, (R)a.scale};
+  const DirectOut<R> out{gout, ok, (R)a.scale, a.st_stream != 0};
   fast_prog<R, DIR, RL, T>(buf, in, out, (const C*)a.tw, (const R*)a.prime_cs, threadIdx.x);
 }
 
@@ -404,7 +419,8 @@ __global__ void __launch_bounds__(T, StreamBounds<R, RL, T>::min_blocks)
     }
     C* buf = buffer(b);
     const FlatIn<R> in{buf};
-    const DirectOut<R> out{gout + (first + i * step) * a.odist, true, (R)a.scale};
+    const DirectOut<R> out{gout + (first + i * step) * a.odist, true, (R)a.scale,
+                           a.st_stream != 0};
     fast_prog<R, DIR, RL, T>(buf, in, out, (const C*)a.tw, (const R*)a.prime_cs, u);
   }
   if (i < nmine && u == 0) {
@@ -426,9 +442,18 @@ template <class RL, int T> __host__ __device__ constexpr int max_values() {
   }
   return m;
 }
+// Threads per tile block: up to 512, or 1024 for ComplexF32 lines of 256
+// threads outside Bluestein (four lines per block, so that a block covers a
+// whole 32-byte sector of each row of a strided axis).
+template <typename R, int T, bool MID> struct TileThreads {
+  static constexpr int value = (sizeof(R) == 4 && T == 256 && !MID) ? 1024 : (T > 512 ? T : 512);
+};
 template <typename R, class RL, int T, bool MID, bool PLAIN> struct TileBounds {
   static constexpr int min_blocks =
-      (!MID && T <= 512 && max_values<RL, T>() <= (sizeof(R) == 4 ? 18 : 9)) ? 2 : 1;
+      (TileThreads<R, T, MID>::value <= 512 && !MID && T <= 512 &&
+       max_values<RL, T>() <= (sizeof(R) == 4 ? 18 : 9))
+          ? 2
+          : 1;
 };
 // Whether a tile launch reserves shared memory for a staged twiddle slice:
 // only four-step passes whose slice follows the second batch level.
@@ -463,7 +488,9 @@ template <typename R, class RL, int T, bool MID, bool PLAIN>
 // 64 registers so two fit per SM -- measured faster than one block with more
 // registers, also where the full-I/O variant then spills a little -- unless a
 // thread holds more than 18 ComplexF32 or 9 ComplexF64 values in some stage.
-__global__ void __launch_bounds__(T > 512 ? T : 512, TileBounds<R, RL, T, MID, PLAIN>::min_blocks)
+// 1024-thread blocks (TileThreads) get the same 64 registers.
+__global__ void __launch_bounds__(TileThreads<R, T, MID>::value,
+                                  TileBounds<R, RL, T, MID, PLAIN>::min_blocks)
     fast_tile_kernel(const LineArgs a) {
   typedef cplx<R> C;
   constexpr int L = prog_len<RL>();
@@ -500,7 +527,7 @@ __global__ void __launch_bounds__(T > 512 ? T : 512, TileBounds<R, RL, T, MID, P
     const int tes = st ? 1 : (int)a.tw_es, toff = st ? 0 : (int)(lt * a.tw_ls);
     const PlainIn<R> in{ib, (int)a.ld.es, tin ? (st ? st : tin) : nullptr, tes, toff, a.tw_dir};
     const PlainOut<R> out{ob, (int)a.st.es, tout ? (st ? st : tout) : nullptr, tes, toff,
-                          a.tw_dir, (R)a.scale, ok};
+                          a.tw_dir, (R)a.scale, ok, a.st_stream != 0};
     if (a.dir1 < 0)
       fast_prog<R, -1, RL, T>(buf, in, out, tw, pcs, u);
     else
@@ -512,7 +539,8 @@ __global__ void __launch_bounds__(T > 512 ? T : 512, TileBounds<R, RL, T, MID, P
                        tin, a.tw_es, lt * a.tw_ls, a.tw_dir};
     const TileOut<R> out{ob, a.st.es, (const C*)a.st.mul, a.st.vn, a.st.ves, l0 * a.st.vls, lt,
                          a.tw_N ? (const C*)a.tw_hi : nullptr, (const C*)a.tw_lo, a.tw_shift,
-                         a.tw_dir, (R)a.scale, ok, tout, a.tw_es, lt * a.tw_ls};
+                         a.tw_dir, (R)a.scale, ok, tout, a.tw_es, lt * a.tw_ls,
+                         a.st_stream != 0};
     if constexpr (MID) {
       fast_prog<R, -1, RL, T>(buf, in, SmemIO{}, tw, pcs, u);
       const C* __restrict__ mid = (const C*)a.mid;
@@ -574,7 +602,7 @@ __global__ void __launch_bounds__(T, TcShape<RL, T>::direct_blocks)
                    (const unsigned char*)a.tcb + (DIR < 0 ? 0 : tc::kTcTableBytes), a.err, u, T);
   const int64_t line = blockIdx.x;  // grid = lines
   const DirectIn<float> in{(const C*)a.in + line * a.idist, true};
-  const DirectOut<float> out{(C*)a.out + line * a.odist, true, (float)a.scale};
+  const DirectOut<float> out{(C*)a.out + line * a.odist, true, (float)a.scale, a.st_stream != 0};
   fast_prog<float, DIR, RL, T, DirectIn<float>, DirectOut<float>, 0, true>(
       (C*)smraw, in, out, (const C*)a.tw, (const float*)a.prime_cs, u, &c);
   tc::tc_end(c);
@@ -617,7 +645,7 @@ __global__ void __launch_bounds__(512, 2) fast_tc_tile_kernel(const LineArgs a) 
                           tin ? (st ? st : tin) : nullptr, tes, toff, a.tw_dir};
   const PlainOut<float> out{(C*)a.out + lb[2 * G + g], (int)a.st.es,
                             tout ? (st ? st : tout) : nullptr, tes, toff, a.tw_dir,
-                            (float)a.scale, ok};
+                            (float)a.scale, ok, a.st_stream != 0};
   const C* tw = (const C*)a.prog.tw;
   const float* pcs = (const float*)a.prime_cs;
   if (a.dir1 < 0)
@@ -667,6 +695,7 @@ static void launch_failure(K k, const char* what, int L, int T, int G, size_t sm
 template <typename R, class RL, int T> struct FastEntry {
   static constexpr int L = prog_len<RL>();
   static constexpr int LPAD = lpad_of(L);
+  static constexpr int TILE_THREADS = TileThreads<R, T, false>::value;
   static cudaError_t launch(int dir, const FastArgs& a, cudaStream_t s) {
     static int set_fwd[64] = {0}, set_bwd[64] = {0};
     const size_t smem = (size_t)a.G * LPAD * sizeof(cplx<R>);
@@ -783,7 +812,8 @@ template <typename R, class RL, int T> struct FastEntry {
                  : (a.plain_io ? fast_tile_kernel<R, RL, T, false, true>
                                : fast_tile_kernel<R, RL, T, false, false>);
     int* set = mid ? set_mid : (a.plain_io ? set_plain : set_full);
-    if (a.G * T > (T > 512 ? T : 512) || (mid && (a.dir1 > 0 || a.dir2 < 0))) {
+    const int max_threads = mid ? TileThreads<R, T, true>::value : TILE_THREADS;
+    if (a.G * T > max_threads || (mid && (a.dir1 > 0 || a.dir2 < 0))) {
       launch_failure(k, "tile launch shape", L, T, a.G, smem, cudaErrorInvalidValue);
       return cudaErrorInvalidValue;
     }

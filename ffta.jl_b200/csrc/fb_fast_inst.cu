@@ -25,7 +25,8 @@ namespace fb {
        : nullptr,                                                              \
    FastEntry<FB_R, RList<__VA_ARGS__>, T>::has_tile_tc                         \
        ? &FastEntry<FB_R, RList<__VA_ARGS__>, T>::launch_tile_tc               \
-       : nullptr}
+       : nullptr,                                                              \
+   FastEntry<FB_R, RList<__VA_ARGS__>, T>::TILE_THREADS}
 
 static const FastFn kTable[] = {
 #include "fb_fast_table.inc"

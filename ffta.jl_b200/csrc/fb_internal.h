@@ -69,6 +69,8 @@ struct LineArgs {
   int* err;             // device flag: set to the radix when a program names one
                         // this kernel has no butterfly for (never traps)
   const void* tcb;      // tensor-core stage: B tables (forward, then backward)
+  int st_stream;        // 1: no later pass of the plan reads the output; the
+                        // specialised kernels store it evict-first
 };
 
 // Shared-memory pitch (elements) of the lines of a tile block.  A warp holds
@@ -105,6 +107,7 @@ struct FastArgs {
   void* const* outs;
   int* err;  // device flag: kErrWaitTimeout when a bulk-copy wait gave up
   const void* tcb;  // tensor-core stage: B tables (forward, then backward)
+  int st_stream;    // 1: store the output evict-first (see LineArgs::st_stream)
 };
 
 // Value of the kernel error flag when a wait on a bulk copy gave up (after
@@ -126,6 +129,8 @@ struct FastFn {
   // (split-BF16 GEMM, FP32 accumulation); nullptr where not available
   cudaError_t (*launch_tc)(int dir, const FastArgs&, cudaStream_t);
   cudaError_t (*launch_tile_tc)(const LineArgs&, cudaStream_t);
+  // threads per block of launch_tile outside Bluestein (G * T at most)
+  int tile_threads;
 };
 
 // Bytes of one direction's B table of the tensor-core radix-16 stage.

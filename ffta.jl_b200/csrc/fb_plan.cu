@@ -454,12 +454,14 @@ namespace fb {
 static int pick_G(const fb_plan_s* P, int L, int T, int Lpad, bool elem_major, int64_t nlines);
 static void apply_tuning(fb_plan_s* P);
 
-// Lines per block of the tile kernel: by its threads (up to 512 per block),
-// and by shared memory -- 100 KB for ComplexF32; ComplexF64 tiles run faster
-// at about 40 KB (more resident blocks per SM, measured).
-static int tile_thread_cap(const FastFn* ff) { return std::max(1, std::max(512, ff->T) / ff->T); }
+// Lines per block of the tile kernel: by its threads (FastFn::tile_threads),
+// and by shared memory -- 100 KB for ComplexF32 (two blocks per SM), up to
+// 220 KB where a block takes more than 512 threads (one block per SM anyway);
+// ComplexF64 tiles run faster at about 40 KB (more resident blocks per SM,
+// measured).
+static int tile_thread_cap(const FastFn* ff) { return std::max(1, ff->tile_threads / ff->T); }
 static int tile_smem_cap(const FastFn* ff, int es) {
-  const size_t budget = es == 8 ? 100 * 1024 : 40 * 1024;
+  const size_t budget = es == 8 ? (ff->tile_threads > 512 ? 220 : 100) * 1024 : 40 * 1024;
   return (int)std::max<size_t>(1, budget / ((size_t)(ff->lpad + 15) * es + 32));
 }
 
@@ -1267,10 +1269,13 @@ static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s
         a.in = (void*)resolve(p.src, offi);
         a.out = resolve(p.dst, offo);
         const bool last = ai + 1 == P->axes.size() && pi + 1 == ax.passes.size();
+        // the last pass's output is read by no later pass: store it evict-first
+        a.st_stream = last ? 1 : 0;
         if (p.fast) {
           FastArgs fa = p.fa;
           fa.in = a.in;
           fa.out = a.out;
+          fa.st_stream = a.st_stream;
           if (last) fa.scale = P->scale;
           // the bulk copies need 16-byte aligned line starts
           const bool st = p.stream && p.fast->launch_stream &&
@@ -2229,7 +2234,7 @@ static std::vector<Shape> pass_shapes(const fb_plan_s* P, const Pass& p) {
       if (G <= cap && (G == G0 || G <= nl) && (size_t)G * p.fast->lpad * es <= smem_max)
         out.push_back({G, T, 0});
   } else if (p.staged) {
-    const int T = p.staged->T, cap = std::max(1, std::max(512, T) / T);
+    const int T = p.staged->T, cap = tile_thread_cap(p.staged);
     for (int G : gs)
       if (G <= cap && (G == G0 || G <= nl) &&
           (size_t)G * (tile_pitch((int)p.staged->lpad, G, es) * es + 32) <= smem_max)
