@@ -50,6 +50,20 @@ template <typename R> __device__ __forceinline__ cplx<R> cmulc(cplx<R> a, cplx<R
   return Sc<R>::mk(Sc<R>::fma(a.x, b.x, Sc<R>::mul(a.y, b.y)),
                    Sc<R>::fma(a.y, b.x, -Sc<R>::mul(a.x, b.y)));
 }
+// Four-step twiddle of element i of a line whose first stage has radix `rad`,
+// from a full table t(k) = w^(k*l) (l: the line's twiddle index).  With
+// nb = L/rad the first stage's butterfly j holds i = j + r*nb; for rad >= 4
+// and r = 4a + c the twiddle is t(i - c*nb) * t(c*nb) (c > 0): a butterfly
+// needs the entries r = 0, 4, 8, ... of its own and the line's three steps
+// t(nb), t(2nb), t(3nb), at the cost of one more rounding.  The specialised
+// and the generic kernels both form exactly this product.
+template <typename R, class Tab>
+__device__ __forceinline__ cplx<R> tw_elem(const Tab& t, int i, int nb, int rad) {
+  if (rad < 4) return t(i);
+  const int c = (i / nb) & 3;
+  const cplx<R> b = t(i - c * nb);
+  return c == 0 ? b : cmul<R>(b, t(c * nb));
+}
 // a * w where w is a forward-direction root; DIR>0 uses conj(w).
 template <typename R, int DIR> __device__ __forceinline__ cplx<R> ctw(cplx<R> a, cplx<R> w) {
   return DIR < 0 ? cmul<R>(a, w) : cmulc<R>(a, w);

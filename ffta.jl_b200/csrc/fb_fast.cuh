@@ -20,7 +20,8 @@
 //                       Bluestein spectrum multiply between a forward and an
 //                       inverse program.
 //
-// The arithmetic -- twiddle table entries, twiddle multiply, butterflies,
+// The arithmetic -- twiddle table entries, twiddle multiply (tw_elem's
+// product for the four-step twiddle on a lean-I/O pass's loads), butterflies,
 // order of stages -- is exactly that of the generic line kernel
 // (fb_line.cuh), so all of them produce the same bits for the same length.
 #pragma once
@@ -194,7 +195,34 @@ template <typename R> struct PlainIn {
     }
     return v;
   }
+  // The twiddles of butterfly j's inputs i = j + r*nb (tw_elem's product):
+  // ceil(RAD/4) entries of its own plus the line's steps t(c*nb), c = 1..3.
+  template <int RAD>
+  __device__ __forceinline__ void fin_bfly(int j, int nb, cplx<R>* v) const {
+    if (!tab) return;
+    if constexpr (RAD < 4) {
+#pragma unroll
+      for (int r = 0; r < RAD; ++r) v[r] = fin(j + r * nb, v[r]);
+    } else {
+      cplx<R> s[4];
+#pragma unroll
+      for (int c = 1; c < 4; ++c) s[c] = tab[c * nb * tab_es + tab_off];
+#pragma unroll
+      for (int a = 0; a < RAD; a += 4) {
+        const cplx<R> b = tab[(j + a * nb) * tab_es + tab_off];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          if (a + c < RAD) {
+            const cplx<R> w = c == 0 ? b : cmul<R>(b, s[c]);
+            v[a + c] = tw_dir < 0 ? cmul<R>(v[a + c], w) : cmulc<R>(v[a + c], w);
+          }
+        }
+      }
+    }
+  }
 };
+template <class In> struct InHasBfly : std::false_type {};
+template <typename R> struct InHasBfly<PlainIn<R>> : std::true_type {};
 template <typename R> struct PlainOut {
   cplx<R>* __restrict__ base;
   int es;
@@ -263,8 +291,12 @@ __device__ __forceinline__ void fast_stage(cplx<R>* buf, const In& in, const Out
     for (int q = 0; q < UM; ++q) {
       const int j = u + q * T;
       if (nb % T == 0 || j < nb) {
+        if constexpr (InHasBfly<In>::value) {
+          in.template fin_bfly<RAD>(j, nb, v[q]);
+        } else {
 #pragma unroll
-        for (int r = 0; r < RAD; ++r) v[q][r] = in.fin(j + r * nb, v[q][r]);
+          for (int r = 0; r < RAD; ++r) v[q][r] = in.fin(j + r * nb, v[q][r]);
+        }
       }
     }
   }

@@ -160,6 +160,18 @@ __device__ __forceinline__ void run_prog(cplx<R>* buf, const StageProg& p, const
 }
 
 // ------------------------------------------------------------ load / store
+// Four-step twiddle of element i on a pass's loads (line twiddle index lt):
+// a lean-I/O pass forms tw_elem's product over the first stage's radix, as the
+// specialised tile kernel does; other passes read the table entry itself.
+template <typename R>
+__device__ __forceinline__ cplx<R> tw_on_load_elem(const LineArgs& a, int64_t lt, int i) {
+  const cplx<R>* __restrict__ t = (const cplx<R>*)a.tw_tab + lt * a.tw_ls;
+  auto at = [&](int k) { return __ldg(t + (int64_t)k * a.tw_es); };
+  if (!a.plain_io) return at(i);
+  const int rad = a.prog.radix[0];
+  return tw_elem<R>(at, i, a.prog.L / rad, rad);
+}
+
 template <typename R>
 __device__ __forceinline__ void load_lines(const LineArgs& a, cplx<R>* sm, const int64_t* lb,
                                            int64_t line0, int tid, int nthr, int u, int gl) {
@@ -180,7 +192,7 @@ __device__ __forceinline__ void load_lines(const LineArgs& a, cplx<R>* sm, const
           v = in[lb[g] + (int64_t)i * io.es];
           if (mul) v = cmul<R>(v, __ldg(mul + vi));
           if (a.tw_on_load) {
-            const C w = __ldg((const C*)a.tw_tab + (int64_t)i * a.tw_es + lb[3 * G + g] * a.tw_ls);
+            const C w = tw_on_load_elem<R>(a, lb[3 * G + g], i);
             v = (a.tw_dir < 0) ? cmul<R>(v, w) : cmulc<R>(v, w);
           }
         }
@@ -199,7 +211,7 @@ __device__ __forceinline__ void load_lines(const LineArgs& a, cplx<R>* sm, const
           v = in[base + (int64_t)i * io.es];
           if (mul) v = cmul<R>(v, __ldg(mul + vi));
           if (a.tw_on_load) {
-            const C w = __ldg((const C*)a.tw_tab + (int64_t)i * a.tw_es + lb[3 * G + g] * a.tw_ls);
+            const C w = tw_on_load_elem<R>(a, lb[3 * G + g], i);
             v = (a.tw_dir < 0) ? cmul<R>(v, w) : cmulc<R>(v, w);
           }
         }

@@ -469,6 +469,19 @@ static int tile_smem_cap(const FastFn* ff, int es) {
 // one is compiled (same arithmetic, direct HBM I/O, lines fastest across a
 // warp).  Bluestein passes need the forward-then-inverse order it implements.
 static void use_tile(const fb_plan_s* P, Pass& p, const std::vector<int>& radices) {
+  // lean I/O when nothing but strides, a full twiddle table and a scale is
+  // needed and every 32-bit offset fits.  Set for generic passes too: a
+  // four-step twiddle on the loads of a lean pass is tw_elem's product in
+  // both kernels, so they keep equal bits.
+  {
+    const int64_t L = p.a.prog.L;
+    const bool small = std::llabs(p.a.ld.es) * L < (int64_t(1) << 31) &&
+                       std::llabs(p.a.st.es) * L < (int64_t(1) << 31) &&
+                       (!p.a.tw_tab || (L * p.a.tw_es + p.a.tw_ls * (int64_t)p.a.nlines) < (int64_t(1) << 31));
+    p.a.plain_io = !p.a.mid && !p.a.ld.mul && !p.a.st.mul && p.a.ld.vn == INT64_MAX &&
+                   p.a.st.vn == INT64_MAX && !(p.a.tw_N && !p.a.tw_tab) && small &&
+                   p.a.ld.count == L && p.a.st.count == L;
+  }
   if (P->flags & 1) return;
   const FastFn* ff = find_fast(P->dtype, p.a.prog.L, radices);
   if (!ff || (int)ff->lpad != p.a.Lpad) return;
@@ -490,15 +503,6 @@ static void use_tile(const fb_plan_s* P, Pass& p, const std::vector<int>& radice
   p.staged = ff;
   p.a.T = T;
   p.a.G = std::max(1, G);
-  // lean I/O when nothing but strides, a full twiddle table and a scale is
-  // needed and every 32-bit offset fits
-  const int64_t L = p.a.prog.L;
-  const bool small = std::llabs(p.a.ld.es) * L < (int64_t(1) << 31) &&
-                     std::llabs(p.a.st.es) * L < (int64_t(1) << 31) &&
-                     (!p.a.tw_tab || (L * p.a.tw_es + p.a.tw_ls * (int64_t)p.a.nlines) < (int64_t(1) << 31));
-  p.a.plain_io = !p.a.mid && !p.a.ld.mul && !p.a.st.mul && p.a.ld.vn == INT64_MAX &&
-                 p.a.st.vn == INT64_MAX && !(p.a.tw_N && !p.a.tw_tab) && small &&
-                 p.a.ld.count == L && p.a.st.count == L;
   if ((P->flags & FB_FLAG_TENSOR_STAGE) && ff->launch_tile_tc && p.a.plain_io) {
     // 512 threads per block: four 128-row tiles of the stage's GEMM
     p.tc = 1;
