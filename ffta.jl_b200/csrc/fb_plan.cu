@@ -494,6 +494,16 @@ static void use_tile(const fb_plan_s* P, Pass& p, const std::vector<int>& radice
   // contiguous runs per DRAM page); contiguous lines: 128-thread blocks
   const int want = em ? thr_cap : std::max(1, 128 / T);
   int G = std::min(std::min(thr_cap, smem_cap), want);
+  // ComplexF64 strided tiles of long lines: up to 4 lines (80 KB) rather
+  // than the 40 KB budget's 2 (four-step columns of 1024: 0.37 -> 0.33 ms
+  // per N = 2^20 x 16 step, autotuned); a lean pass that also loads the
+  // four-step twiddle takes half the lines (its table loads add latency
+  // per line: N = 2^20 C32 pass 2 and the short rows of 27648, 19683)
+  if (em && es == 16 && G < 4) {
+    const int g80 = (int)((80 * 1024) / ((size_t)(ff->lpad + 15) * es + 32));
+    G = std::max(G, std::min(std::min(4, thr_cap), g80));
+  }
+  if (em && p.a.tw_on_load && p.a.plain_io && G >= 4) G /= 2;
   const int64_t nl = std::max<int64_t>(1, p.a.nlines);
   while (G > 1 && G / 2 >= nl) G /= 2;
   // lines contiguous on load: at least about four blocks per SM when the
