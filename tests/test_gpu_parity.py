@@ -359,6 +359,28 @@ def test_config2_batched(N, dtype):
             assert e <= 1e-6
 
 
+@pytest.mark.parametrize("N,B,dtype", [(2 ** 15, 8, np.complex64), (2 ** 20, 2, np.complex64),
+                                       (27648, 6, np.complex64), (2 ** 14 * 3, 4, np.complex128),
+                                       (2 ** 20, 2, np.complex128)])
+def test_four_step_specialised_equals_generic(N, B, dtype):
+    """Four-step passes on the specialised tile kernels give the generic
+    kernel's bits: both take the twiddle on a lean pass's loads as the same
+    product of two table entries."""
+    import torch
+    rng = np.random.default_rng(N + B)
+    x = torch.from_numpy(crandn(rng, (B, N), dtype)).cuda()
+    for planner in (F.plan_fft, F.plan_bfft):
+        fast = planner(x.T, 1)
+        gen = planner(x.T, 1, _flags=F.FB_FLAG_GENERIC_ONLY)
+        df, dg = fast.describe(x.T), gen.describe(x.T)
+        assert "FOUR" in df and "tile" in df and "tile" not in dg, (df, dg)
+        a = (fast * x.T).T.cpu().numpy()
+        b = (gen * x.T).T.cpu().numpy()
+        assert np.array_equal(a, b), (N, planner.__name__, df, dg)
+        ref = oracle.fft_batched(x.cpu().numpy().astype(np.complex128), fast.dir, nthreads=NTHR)
+        assert relerr(a, ref) <= tol(dtype, N)
+
+
 @pytest.mark.parametrize("N,B", [(1009, 64), (65537, 16), (1000003, 1), (2 ** 8 * 4099, 4)])
 def test_config3_bluestein_tone(N, B):
     rng = np.random.default_rng(N)
