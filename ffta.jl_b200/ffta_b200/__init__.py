@@ -203,6 +203,9 @@ class FFTAPlan_cx:
         self.BLUESTEIN_CUTOFF = cutoff
         self.scale = scale
         self._cplans = {}
+        # layouts of (x, y) device tensors that passed every check of mul_
+        # without a copy -> their C plan (owned by _cplans)
+        self._fast = {}
 
     # -- AbstractFFTs surface
     def size(self, i=None):
@@ -341,8 +344,43 @@ def size(p: FFTAPlan_cx, i=None):
     return p.size(i)
 
 
+def _fast_key(y, x):
+    """Layout key of two complex CUDA tensors (shapes, strides, type,
+    devices), or None for anything else."""
+    if not (_is_torch(x) and _is_torch(y)):
+        return None
+    dt = x.dtype
+    if dt is not y.dtype or not dt.is_complex or not x.is_cuda or not y.is_cuda:
+        return None
+    return (x.shape, x.stride(), y.shape, y.stride(), dt, x.device.index, y.device.index)
+
+
+def _execute_device(h, x, y):
+    """fb_execute on the current stream of x's device."""
+    torch = _torch()
+    dev = x.device
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    args = (h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(y.data_ptr()), ctypes.c_void_p(stream))
+    if dev.index == torch.cuda.current_device():
+        _check(lib.fb_execute(*args))
+    else:
+        with torch.cuda.device(dev):
+            _check(lib.fb_execute(*args))
+
+
 def mul_(y, p: FFTAPlan_cx, x):
-    """LinearAlgebra.mul!(y, p, x) with FFTA's argument checks (src/plan.jl:157-285)."""
+    """LinearAlgebra.mul!(y, p, x) with FFTA's argument checks (src/plan.jl:157-285).
+
+    Device tensors laid out like an earlier call's that passed those checks
+    without a copy (same shapes, strides, type and devices) go straight to
+    the plan that call used: the checks depend on nothing else."""
+    fk = _fast_key(y, x)
+    if fk is not None:
+        h = p._fast.get(fk)
+        if h is not None:
+            _execute_device(h, x, y)
+            return y
+    x_arg = x
     x = p._accept(x)
     if _is_torch(y) != _is_torch(x):
         raise ArgumentError("input and output must both be host arrays or both device tensors")
@@ -401,13 +439,11 @@ def mul_(y, p: FFTAPlan_cx, x):
         y = _similar(y)
     h = p._cplan(y, x)
     if _is_torch(x):
-        torch = _torch()
         if not x.is_cuda or not y.is_cuda:
             raise ArgumentError("torch tensors must live on a CUDA device")
-        stream = torch.cuda.current_stream(x.device).cuda_stream
-        with torch.cuda.device(x.device):
-            _check(lib.fb_execute(h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(y.data_ptr()),
-                                  ctypes.c_void_p(stream)))
+        _execute_device(h, x, y)
+        if fk is not None and x is x_arg and y is y_target:
+            p._fast[fk] = h
     else:
         _check(lib.fb_execute_host(h, ctypes.c_void_p(x.ctypes.data), ctypes.c_void_p(y.ctypes.data),
                                    None))

@@ -310,6 +310,29 @@ def test_host_pipeline_matches_device(n, B, dtype):
         assert np.array_equal(host, dev)
 
 
+def test_repeated_calls_reuse_the_checked_plan():
+    """A repeated mul_ on tensors laid out like an earlier call's skips the
+    argument checks and reuses that call's plan (same bits); any other layout
+    or element type still meets every check."""
+    import torch
+    rng = np.random.default_rng(5)
+    x = torch.from_numpy(crandn(rng, (6, 1000), np.complex64)).cuda().T  # 1000 x 6, column-major
+    y = torch.empty_like(x)
+    p = F.plan_fft(x, 1)
+    first = F.mul_(y, p, x).cpu().clone()
+    assert len(p._fast) == 1
+    for _ in range(3):
+        assert torch.equal(F.mul_(y, p, x).cpu(), first)
+    ref = oracle.fft_nd(x.cpu().numpy(), 1, -1, prec="f64", nthreads=NTHR)
+    assert relerr(first.numpy(), ref) <= tol(np.complex64, 1000)
+    short = x[:999]
+    with pytest.raises(F.DimensionMismatch):
+        F.mul_(torch.empty_like(short), p, short)
+    with pytest.raises(F.ArgumentError):
+        F.mul_(y.to(torch.complex128), p, x.to(torch.complex128))
+    assert len(p._fast) == 1
+
+
 def test_in_place_and_strided():
     import torch
     rng = np.random.default_rng(5)
