@@ -221,18 +221,19 @@ def test_2d_regions_bitwise(n):
             assert np.array_equal(a[tuple(sl)], ref)
 
 
-@pytest.mark.parametrize("n", [1024, 4096])
-def test_long_strided_axis(n):
+@pytest.mark.parametrize("n,dtype", [(1024, np.complex64), (4096, np.complex64),
+                                     (1024, np.complex128), (4096, np.complex128)])
+def test_long_strided_axis(n, dtype):
     """Long strided lines take a four-step split (tolerance vs the contiguous
     schedule); FB_FLAG_SAME_SCHEDULE_STRIDED restores bitwise equality."""
     import torch
     rng = np.random.default_rng(n)
-    X = torch.from_numpy(crandn(rng, (n, 48), np.complex64)).cuda()  # column axis 1 strided
+    X = torch.from_numpy(crandn(rng, (n, 48), dtype)).cuda()  # column axis 1 strided
     cont = F.fft(X.T.contiguous(), 2).T.cpu().numpy()  # rows are contiguous lines
     y = F.fft(X, 1).cpu().numpy()
     ref = oracle.fft_nd(X.cpu().numpy(), 1, -1, prec="f64", nthreads=NTHR)
-    assert relerr(y, ref) <= tol(np.complex64, n)
-    assert relerr(cont, ref) <= tol(np.complex64, n)
+    assert relerr(y, ref) <= tol(dtype, n)
+    assert relerr(cont, ref) <= tol(dtype, n)
     p = F.plan_fft(X, 1, _flags=F.FB_FLAG_SAME_SCHEDULE_STRIDED)
     assert np.array_equal((p * X).cpu().numpy(), cont), p.describe(X)
 
