@@ -61,8 +61,38 @@ EXTRA = [
 ]
 
 
+SPEC_HBM_GBS = 8000.0  # B200 HBM3e specification, GB/s
+
+# DRAM traffic of one launch of the headline kernel (fast_direct_kernel, C32
+# N=4096): dram__bytes_read.sum + dram__bytes_write.sum from an ncu capture of
+# three back-to-back launches at batch 4096 (inputs and outputs of 134 MB,
+# each larger than L2) with --cache-control none, taken from the third
+# launch, so that the write-back of an earlier launch's output still held in
+# L2 is counted like the steady state of the timed loop.  Traffic grows with
+# the columns, so the bench scales it by its batch / 4096.
+HEADLINE_TRAFFIC = (4096, 134.27e6 + 84.74e6,
+                    "ncu dram__bytes_read.sum + dram__bytes_write.sum, batch-4096 launch")
+
+
 def flops(n, b):
     return 5.0 * n * np.log2(n) * b
+
+
+def spot_rel_l2(x, y, dims, max_cols=3):
+    """rel-L2 of a device result against the FP64 oracle: up to `max_cols`
+    transforms of the batch (first, middle, last).  x, y: torch tensors shaped
+    (batch, reversed dims), i.e. Julia's column-major (dims..., batch)."""
+    import oracle
+    b = x.shape[0]
+    cols = sorted({0, b // 2, b - 1})[:max_cols]
+    xs = x[cols].cpu().numpy().astype(np.complex128)
+    ys = y[cols].cpu().numpy().astype(np.complex128)
+    nthr = os.cpu_count() or 1
+    if len(dims) == 1:
+        ref = oracle.fft_batched(xs, -1, nthreads=nthr)
+    else:
+        ref = np.stack([oracle.fft(np.asfortranarray(v.T), nthreads=nthr).T for v in xs])
+    return float(np.linalg.norm(ys - ref) / np.linalg.norm(ref))
 
 
 def peaks():
@@ -165,11 +195,50 @@ def run_reference(args):
                                    f"{nthreads} threads (FFTA itself is single-threaded)"},
         "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
-        "note": "FFTA.jl (Julia) is not installed on this image; the reference arm runs the "
-                "C++ restatement of FFTA's algorithm (oracle/ffta_oracle.cpp)",
+        "note": julia_probe(),
     }
     print(json.dumps(line))
     return 0
+
+
+def julia_probe():
+    """Whether FFTA.jl itself could be timed on this host: a `julia` binary on
+    PATH and FFTA's sources.  The sources of the reference are not shipped with
+    this repository, so the reference arm times the C++ restatement of FFTA's
+    algorithm (oracle/ffta_oracle.cpp) either way; the probe's answer is
+    recorded in the line."""
+    import shutil
+    jl = shutil.which("julia")
+    if jl is None:
+        return ("julia: not found on PATH on this host, so FFTA.jl cannot run here; the "
+                "reference arm times the C++ restatement of FFTA's algorithm "
+                "(oracle/ffta_oracle.cpp)")
+    try:
+        ver = subprocess.run([jl, "--version"], capture_output=True, text=True,
+                             timeout=60).stdout.strip()
+    except (OSError, subprocess.TimeoutExpired) as e:
+        ver = f"unusable ({e})"
+    return (f"julia found at {jl} ({ver}), but FFTA.jl's sources are not present on this "
+            "host; the reference arm times the C++ restatement of FFTA's algorithm "
+            "(oracle/ffta_oracle.cpp)")
+
+
+def launch_command(gpus, argv, port=None, script=None):
+    """torchrun command that re-runs this script (or `script`) with one
+    process per GPU, rendezvous on 127.0.0.1."""
+    port = port or 29500 + (os.getpid() % 1000)
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+            f"--nproc-per-node={gpus}", "--master-addr", "127.0.0.1",
+            "--master-port", str(port), script or os.path.abspath(__file__)] + list(argv)
+
+
+def maybe_launch(gpus, argv):
+    """`bench.py --gpus N` started without torchrun (no WORLD_SIZE in the
+    environment) starts its N ranks itself; returns their exit code, or None
+    when this process is already a rank (or N is 1)."""
+    if gpus <= 1 or "WORLD_SIZE" in os.environ:
+        return None
+    return subprocess.run(["timeout", "-k", "60", "1800"] + launch_command(gpus, argv)).returncode
 
 
 def main():
@@ -191,6 +260,9 @@ def main():
                     help="time one of the `extra` configurations instead of the headline "
                          "(for profiling captures): " + ", ".join(e[0] for e in EXTRA))
     args = ap.parse_args()
+    rc = maybe_launch(args.gpus, sys.argv[1:])
+    if rc is not None:
+        return rc
     if args.impl == "reference":
         return run_reference(args)
     args.warmup = max(args.warmup, 3)
@@ -272,15 +344,7 @@ def main():
     peak, peak_kind = peaks()
 
     # accuracy spot check of this run against the FP64 oracle on a few columns
-    import oracle
-    cols = sorted({0, batch // 2, batch - 1})
-    xs = x[cols].cpu().numpy().astype(np.complex128)
-    ys = y[cols].cpu().numpy()
-    if len(dims) == 1:
-        ref = oracle.fft_batched(xs, -1, nthreads=4)
-    else:
-        ref = np.stack([oracle.fft(np.asfortranarray(v.T), nthreads=4).T for v in xs])
-    rel = float(np.linalg.norm(ys - ref) / np.linalg.norm(ref))
+    rel = spot_rel_l2(x, y, dims)
 
     # e2e: through the C ABI with host buffers (pinned), copies inside the timed region
     hx = x.cpu().pin_memory()
@@ -327,10 +391,11 @@ def main():
             t = e0.elapsed_time(e1) / reps
             en = int(np.prod(dims_))
             fl = 5.0 * en * np.log2(en) * b2
+            gbs = 2.0 * en * b2 * ees / (t * 1e-3) / 1e9
             extra[label_] = {
-                "ms": t, "GFLOP/s": fl / (t * 1e-3) / 1e9,
-                "GB/s": 2.0 * en * b2 * ees / (t * 1e-3) / 1e9,
-                "frac_of_hbm": 2.0 * en * b2 * ees / (t * 1e-3) / 1e9 / peaks()[0],
+                "ms": t, "GFLOP/s": fl / (t * 1e-3) / 1e9, "GB/s": gbs,
+                "frac_of_hbm": gbs / peaks()[0], "frac_of_spec_8tbs": gbs / SPEC_HBM_GBS,
+                "rel_l2_vs_fp64_oracle": spot_rel_l2(xe, ye, dims_),
                 "schedule": pe.describe(xj)}
             del xe, ye, pe, xj, yj
 
@@ -404,15 +469,13 @@ def main():
                                  "sample": f"256 transforms of N={N} on one thread "
                                            f"(FFTA itself is single-threaded), {dt1:.2f} s"}}
 
-    # DRAM bytes per launch of the headline kernel from one ncu capture of the
-    # same kernel at batch 4096 (profiles/fast_direct_c32_n4096.md: 134.27 MB
-    # read + 84.74 MB written), scaled by 16384/4096; writes still in L2 when
-    # that launch ended are not counted there
+    # DRAM bytes per launch of the headline kernel, measured by ncu (see
+    # HEADLINE_TRAFFIC) and scaled from its batch to this launch's batch
     traffic, traffic_note = None, None
-    if label == "headline" and batch == 16384 and not args.tensor_stage:
-        traffic = 4 * (134.27e6 + 84.74e6)
-        traffic_note = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the batch-4096 "
-                        "launch, scaled x4 (profiles/fast_direct_c32_n4096.md)")
+    if label == "headline" and not args.tensor_stage:
+        tb, tbytes, tnote = HEADLINE_TRAFFIC
+        traffic = tbytes * batch / tb
+        traffic_note = tnote + f"; scaled by {batch}/{tb} columns"
     if rank == 0:
         wl = (f"batched C32 forward FFT, N={N}, {BATCH} contiguous columns per GPU"
               if label == "headline" else f"{label} forward FFT")
@@ -427,6 +490,7 @@ def main():
                        "schedule": p.describe(xt)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
+                         "frac_of_spec_8tbs": achieved / SPEC_HBM_GBS,
                          "alg_bytes_per_launch": alg_bytes, "traffic": traffic,
                          "traffic_source": traffic_note},
             "hbm_gbs": achieved,

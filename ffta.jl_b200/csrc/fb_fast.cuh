@@ -439,7 +439,7 @@ __global__ void __launch_bounds__(T, StreamBounds<R, RL, T>::min_blocks)
   int64_t i = 0;
   for (; i < nmine; ++i) {
     const int b = (int)(i % NBUF);
-    const bool got = mbar_wait(bar + b, (uint32_t)((i / NBUF) & 1));
+    const bool got = mbar_wait(bar + b, (uint32_t)((i / NBUF) & 1), a.wait_ns);
     // every thread has also finished line i-1, so its buffer is free
     if (!__syncthreads_and(got)) break;
     const int64_t nx = i + NBUF - 1;
@@ -457,9 +457,10 @@ __global__ void __launch_bounds__(T, StreamBounds<R, RL, T>::min_blocks)
   }
   if (i < nmine && u == 0) {
     // gave up on line i: flag it, then let the copies still in flight land
+    // (waiting at least the default limit, whatever the launch's limit)
     if (a.err) atomicExch(a.err, kErrWaitTimeout);
     for (int64_t k = i; k < nmine && k < i + NBUF - 1; ++k)
-      mbar_wait(bar + (int)(k % NBUF), (uint32_t)((k / NBUF) & 1));
+      mbar_wait(bar + (int)(k % NBUF), (uint32_t)((k / NBUF) & 1), drain_limit(a.wait_ns));
   }
 }
 
@@ -631,7 +632,8 @@ __global__ void __launch_bounds__(T, TcShape<RL, T>::direct_blocks)
   const int u = threadIdx.x;
   const tc::TcCtx c =
       tc::tc_begin(smraw, b, bar, slot,
-                   (const unsigned char*)a.tcb + (DIR < 0 ? 0 : tc::kTcTableBytes), a.err, u, T);
+                   (const unsigned char*)a.tcb + (DIR < 0 ? 0 : tc::kTcTableBytes), a.err, u, T,
+                   a.wait_ns);
   const int64_t line = blockIdx.x;  // grid = lines
   const DirectIn<float> in{(const C*)a.in + line * a.idist, true};
   const DirectOut<float> out{(C*)a.out + line * a.odist, true, (float)a.scale, a.st_stream != 0};
@@ -666,7 +668,7 @@ __global__ void __launch_bounds__(512, 2) fast_tc_tile_kernel(const LineArgs a) 
   // (tc_begin's barrier publishes lb)
   const tc::TcCtx c = tc::tc_begin(
       smraw, b, bar, slot, (const unsigned char*)a.tcb + (a.dir1 < 0 ? 0 : tc::kTcTableBytes),
-      a.err, g + G * u, G * T);
+      a.err, g + G * u, G * T, a.wait_ns);
   const int64_t lt = lb[3 * G + g];
   const C* tin = a.tw_on_load ? (const C*)a.tw_tab : nullptr;
   const C* tout = a.tw_on_load ? nullptr : (const C*)a.tw_tab;

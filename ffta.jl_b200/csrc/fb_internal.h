@@ -71,6 +71,8 @@ struct LineArgs {
   const void* tcb;      // tensor-core stage: B tables (forward, then backward)
   int st_stream;        // 1: no later pass of the plan reads the output; the
                         // specialised kernels store it evict-first
+  uint64_t wait_ns;     // limit of a wait on the block's own asynchronous
+                        // work (tensor-core products); 0: kWaitNsDefault
 };
 
 // Shared-memory pitch (elements) of the lines of a tile block.  A warp holds
@@ -108,11 +110,19 @@ struct FastArgs {
   int* err;  // device flag: kErrWaitTimeout when a bulk-copy wait gave up
   const void* tcb;  // tensor-core stage: B tables (forward, then backward)
   int st_stream;    // 1: store the output evict-first (see LineArgs::st_stream)
+  uint64_t wait_ns; // limit of a wait on the block's own bulk copies or
+                    // tensor-core products; 0: kWaitNsDefault
 };
 
-// Value of the kernel error flag when a wait on a bulk copy gave up (after
-// about a second); the kernel then stops early and leaves its output partial.
+// Value of the kernel error flag when a wait on a bulk copy or on tensor-core
+// products gave up; the kernel then stops early and leaves its output partial.
 constexpr int kErrWaitTimeout = -1;
+// Default limit of such a wait (ns).  After giving up, a block still waits up
+// to this long (never less) for the copies and products it has in flight
+// before it touches their shared or tensor memory again, frees it or exits.
+constexpr uint64_t kWaitNsDefault = 1000000000ull;
+// The limit a launch uses: fb_set_wait_limit's value, 0 for the default.
+uint64_t wait_limit_ns();
 
 // One specialised length: its radix program, threads per line, launcher and
 // padded shared-memory elements per line.

@@ -19,6 +19,8 @@
 // Sharing: every call on a device uses the same two arrays and leaves its
 // contents behind.  Nothing in them has to start at zero: each call rewrites
 // the tables it reads, and pass 1 writes every scratch element pass 2 reads.
+// In place (in == out) is allowed: pass 1 reads all of the input into the
+// scratch before pass 2, on the same stream, writes the output.
 // Calls whose work overlaps on the GPU (different streams, or different host
 // threads without ordering between them) race on the arrays and give wrong
 // results; run them on one stream or otherwise serialise them.
@@ -140,9 +142,13 @@ static int64_t stage_tables(float2* dst, const std::vector<int>& rad, int* off, 
 
 static int noalloc_run(const void* in, void* out, int64_t n, int64_t batch, int dir,
                        cudaStream_t stream) {
-  if (n <= 0 || batch < 0) {
+  if (n <= 0) {
     noalloc_error("Array length must be strictly positive");
     return FB_ERR_DIMENSION_MISMATCH;
+  }
+  if (batch < 0) {
+    noalloc_error("fb_execute_noalloc_c32: batch must be >= 0, got " + std::to_string(batch));
+    return FB_ERR_ARGUMENT;
   }
   if (dir != FB_FORWARD && dir != FB_BACKWARD) {
     noalloc_error("direction must be -1 or +1");
@@ -166,10 +172,15 @@ static int noalloc_run(const void* in, void* out, int64_t n, int64_t batch, int 
   }
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev >= 64) {
+  if (e != cudaSuccess) {
     noalloc_error(std::string("no usable CUDA device: ") + cudaGetErrorString(e));
     cudaGetLastError();
     return FB_ERR_CUDA;
+  }
+  if (dev >= 64) {
+    noalloc_error("fb_execute_noalloc_c32: device index " + std::to_string(dev) +
+                  " is beyond the 64 devices whose array addresses it caches");
+    return FB_ERR_UNSUPPORTED;
   }
   NoallocDev d;
   {

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -41,6 +42,10 @@ namespace fb {
 
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+// fb_set_wait_limit's value (0: the kernels' default limit).
+static std::atomic<uint64_t> g_wait_ns{0};
+uint64_t wait_limit_ns() { return g_wait_ns.load(std::memory_order_relaxed); }
 
 struct FbError {
   int code;
@@ -1285,11 +1290,13 @@ static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s
         const bool last = ai + 1 == P->axes.size() && pi + 1 == ax.passes.size();
         // the last pass's output is read by no later pass: store it evict-first
         a.st_stream = last ? 1 : 0;
+        a.wait_ns = wait_limit_ns();
         if (p.fast) {
           FastArgs fa = p.fa;
           fa.in = a.in;
           fa.out = a.out;
           fa.st_stream = a.st_stream;
+          fa.wait_ns = a.wait_ns;
           if (last) fa.scale = P->scale;
           // the bulk copies need 16-byte aligned line starts
           const bool st = p.stream && p.fast->launch_stream &&
@@ -1581,6 +1588,12 @@ int fb_kernel_error_flag(int* value, int reset) {
   });
 }
 
+int fb_set_wait_limit(int64_t ns) {
+  g_wait_ns.store(ns > 0 ? (uint64_t)ns : 0, std::memory_order_relaxed);
+  set_last_error("");
+  return FB_OK;
+}
+
 const char* fb_last_error(void) { return g_last_error.c_str(); }
 const char* fb_version(void) { return FB_VERSION; }
 
@@ -1755,6 +1768,7 @@ struct fb_server_s {
   std::vector<std::pair<cudaEvent_t, cudaGraphExec_t>> graph_retiring;
   int64_t graph_clock = 0, st_graph_launches = 0, st_graph_captures = 0;
   int64_t st_launches = 0, st_desc_launches = 0, st_requests = 0, st_max_queue = 0;
+  int64_t st_cancelled = 0;
   double st_max_admitted = 0;
   ~fb_server_s() {
     for (auto& g : graph_of) cudaGraphExecDestroy(g.second.exec);
@@ -2103,13 +2117,22 @@ int fb_server_submit(fb_server srv, int64_t n, int dtype, int dir, int64_t batch
     if (dir != FB_FORWARD && dir != FB_BACKWARD) fail(FB_ERR_ARGUMENT, "direction must be -1 or +1");
     if (batch < 1 || !in || !out) fail(FB_ERR_ARGUMENT, "bad batch or data pointer");
     // plans are made at submission (tables resident); bytes = data + scratch
-    fb_plan_s* T = srv_template(srv, n, dtype, dir);
     double bytes = 2.0 * (double)n * (double)batch * elem_bytes(dtype);
+    auto refuse = [&]() {
+      std::ostringstream m;
+      m << "request needs " << (int64_t)bytes << " device bytes (input, output, scratch), above "
+        << "the server's budget of " << (int64_t)srv->budget;
+      fail(FB_ERR_OUT_OF_MEMORY, m.str());
+    };
+    if (bytes > srv->budget) refuse();  // before any plan (and its scratch) is made
+    fb_plan_s* T = srv_template(srv, n, dtype, dir);
     // large single-pass requests run their own plan (specialised kernels) on
     // a plan stream; small ones are packed into descriptor launches
     const bool packed = srv_single_pass(T) && n * batch < kPackedMaxElems;
     const SrvShape* shape = packed ? srv_shape(srv, T, dtype) : nullptr;
     if (!shape) bytes += (double)plan_scratch_bytes(srv_multi(srv, n, dtype, dir, batch));
+    // a request that could never be admitted is refused now, not queued for good
+    if (bytes > srv->budget) refuse();
     SrvReq r{srv->next_ticket++, n, batch, dtype, dir, in, out, bytes, shape};
     srv->pending.push_back(r);
     srv->st_requests += 1;
@@ -2147,6 +2170,20 @@ int fb_server_poll(fb_server srv, int64_t max, int64_t* tickets, double* done_ms
   });
 }
 
+int fb_server_cancel(fb_server srv, int64_t ticket) {
+  return guard([&] {
+    if (!srv) fail(FB_ERR_ARGUMENT, "null argument");
+    for (auto it = srv->pending.begin(); it != srv->pending.end(); ++it) {
+      if (it->ticket != ticket) continue;
+      srv->pending.erase(it);
+      srv->st_cancelled += 1;
+      return;
+    }
+    fail(FB_ERR_ARGUMENT, "ticket " + std::to_string(ticket) +
+                              " is not waiting: unknown, already dispatched or completed");
+  });
+}
+
 int fb_server_wait(fb_server srv) {
   return guard([&] {
     if (!srv) fail(FB_ERR_ARGUMENT, "null argument");
@@ -2160,11 +2197,11 @@ int fb_server_wait(fb_server srv) {
 int fb_server_stats(fb_server srv, int64_t* out, int nout) {
   return guard([&] {
     if (!srv || !out) fail(FB_ERR_ARGUMENT, "null argument");
-    const int64_t v[8] = {srv->st_requests, srv->st_launches, srv->st_desc_launches,
+    const int64_t v[9] = {srv->st_requests, srv->st_launches, srv->st_desc_launches,
                           srv->st_max_queue, (int64_t)srv->st_max_admitted,
                           (int64_t)(srv->templ.size() + srv->multi.size()),
-                          srv->st_graph_launches, srv->st_graph_captures};
-    for (int i = 0; i < nout && i < 8; ++i) out[i] = v[i];
+                          srv->st_graph_launches, srv->st_graph_captures, srv->st_cancelled};
+    for (int i = 0; i < nout && i < 9; ++i) out[i] = v[i];
   });
 }
 

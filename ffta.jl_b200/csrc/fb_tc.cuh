@@ -54,15 +54,22 @@ __device__ __forceinline__ uint64_t global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// Wait for phase `parity` of *b for at most ~1 s; false if it gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
+// Wait for phase `parity` of *b for at most `limit_ns` (0: kWaitNsDefault);
+// false if it gave up.  The iteration count is bounded as well.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, uint64_t limit_ns = 0) {
   if (mbar_test(b, parity)) return true;
+  const uint64_t lim = limit_ns ? limit_ns : kWaitNsDefault;
   const uint64_t t0 = global_ns();
   for (uint32_t it = 0; it < (1u << 30); ++it) {
+    if (global_ns() - t0 >= lim) return false;
     if (mbar_test(b, parity)) return true;
-    if ((it & 63) == 63 && global_ns() - t0 > 1000000000ull) return false;
   }
   return false;
+}
+// The limit of a drain: the wait for a block's own copies or products still
+// in flight after an earlier wait gave up -- never shorter than the default.
+__device__ __forceinline__ uint64_t drain_limit(uint64_t limit_ns) {
+  return limit_ns > kWaitNsDefault ? limit_ns : kWaitNsDefault;
 }
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
                                           uint64_t* b) {
@@ -218,6 +225,7 @@ struct TcCtx {
   int* err;
   int t;   // block-linear thread id (= row of A and D)
   int nt;  // threads of the block: a multiple of 128, at most 512
+  uint64_t wait_ns;  // limit of the wait for the products (0: default)
 };
 
 // Tensor-memory columns a block of NT threads allocates: two 32-column
@@ -227,8 +235,12 @@ __host__ __device__ constexpr uint32_t tc_cols(int NT) {
 }
 
 // The radix-16 DFT of v (this thread's butterfly).  Every thread of the
-// block calls it once.  If the MMAs do not complete within about a second the
-// error flag is set to kErrWaitTimeout and v becomes zero.
+// block calls it once.  If the MMAs do not complete within the wait limit
+// (about a second by default) the error flag is set to kErrWaitTimeout and v
+// becomes zero -- but only after a second, longer wait (drain_limit) for the
+// products in flight, so that the block never rewrites the A region (its
+// line buffers) or frees tensor memory while the tensor core may still use
+// them.
 __device__ __forceinline__ void tc_dft16(cplx<float> (&v)[16], const TcCtx& c) {
   const int t = c.t;
   // 1. A row t, 16 bytes (8 BF16) per store
@@ -269,7 +281,7 @@ __device__ __forceinline__ void tc_dft16(cplx<float> (&v)[16], const TcCtx& c) {
     mma_commit(c.bar);
   }
   // 3. wait for the products, then each warp reads its 32 rows
-  const bool got = mbar_wait(c.bar, 0);
+  const bool got = mbar_wait(c.bar, 0, c.wait_ns);
   const bool ok = __syncthreads_and(got);
   fence_after_sync();
   if (ok) {
@@ -286,6 +298,10 @@ __device__ __forceinline__ void tc_dft16(cplx<float> (&v)[16], const TcCtx& c) {
     for (int r = 0; r < 16; ++r) v[r].y = __fadd_rn(d[r], e[r]);
   } else {
     if (t == 0 && c.err) atomicExch(c.err, kErrWaitTimeout);
+    // drain: the products complete before anyone reuses A or the columns
+    mbar_wait(c.bar, 0, drain_limit(c.wait_ns));
+    __syncthreads();
+    fence_after_sync();
 #pragma unroll
     for (int r = 0; r < 16; ++r) v[r] = Sc<float>::mk(0.f, 0.f);
   }
@@ -298,7 +314,7 @@ __device__ __forceinline__ void tc_dft16(cplx<float> (&v)[16], const TcCtx& c) {
 // last tensor-memory load of the block, free the columns (warp 0).
 __device__ __forceinline__ TcCtx tc_begin(unsigned char* a, unsigned char* b, uint64_t* bar,
                                           uint32_t* taddr_slot, const void* table, int* err,
-                                          int t, int nt) {
+                                          int t, int nt, uint64_t wait_ns) {
   for (int i = t; i < kTcTableBytes / 16; i += nt) ((uint4*)b)[i] = ((const uint4*)table)[i];
   if (t == 0) {
     mbar_init(bar, 1);
@@ -311,7 +327,7 @@ __device__ __forceinline__ TcCtx tc_begin(unsigned char* a, unsigned char* b, ui
   fence_before_sync();
   __syncthreads();
   fence_after_sync();
-  return TcCtx{a, b, bar, *taddr_slot, err, t, nt};
+  return TcCtx{a, b, bar, *taddr_slot, err, t, nt, wait_ns};
 }
 __device__ __forceinline__ void tc_end(const TcCtx& c) {
   fence_before_sync();

@@ -113,6 +113,9 @@ def _promote(x):
     kind = _complex_dtype_name(x)
     if _is_torch(x):
         torch = _torch()
+        # torch keeps conj() and negation of a view as flags on the tensor,
+        # not in its storage; the kernels read the storage, so materialise them
+        x = x.resolve_conj().resolve_neg()
         want = torch.complex64 if kind == "c64" else torch.complex128
         return x if x.dtype == want else x.to(want)
     x = np.asarray(x)
@@ -127,6 +130,8 @@ def _shape(x):
 def _elem_strides(x):
     """Element strides of x, or None when x needs a copy (negative/odd strides)."""
     if _is_torch(x):
+        if x.is_conj() or x.is_neg():
+            return None  # lazily conjugated/negated view: the storage is not the values
         st = tuple(int(s) for s in x.stride())
         return None if any(s < 0 for s in st) else st
     item = x.itemsize
@@ -142,6 +147,8 @@ def _similar(x):
     """Julia's similar(x): a new array of the same shape and element type."""
     if _is_torch(x):
         torch = _torch()
+        if x.is_conj() or x.is_neg():
+            return torch.empty(x.shape, dtype=x.dtype, device=x.device)
         if x.is_contiguous():
             return torch.empty_like(x, memory_format=torch.contiguous_format)
         # keep a dense layout with the same dim order when x is dense
@@ -351,6 +358,8 @@ def _fast_key(y, x):
         return None
     dt = x.dtype
     if dt is not y.dtype or not dt.is_complex or not x.is_cuda or not y.is_cuda:
+        return None
+    if x.is_conj() or x.is_neg() or y.is_conj() or y.is_neg():
         return None
     return (x.shape, x.stride(), y.shape, y.stride(), dt, x.device.index, y.device.index)
 

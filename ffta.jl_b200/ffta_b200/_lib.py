@@ -48,6 +48,7 @@ SIGNATURES = {
     "fb_plan_describe": ([_vp, ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
     "fb_plan_destroy": ([_vp], ctypes.c_int),
     "fb_kernel_error_flag": ([ctypes.POINTER(ctypes.c_int), ctypes.c_int], ctypes.c_int),
+    "fb_set_wait_limit": ([_i64], ctypes.c_int),
     "fb_execute_noalloc_c32": ([_vp, _vp, _i64, _i64, ctypes.c_int, _vp], ctypes.c_int),
     "fb_server_create": ([_plan_p, ctypes.c_double, ctypes.c_int, ctypes.c_uint32], ctypes.c_int),
     "fb_server_submit": ([_vp, _i64, ctypes.c_int, ctypes.c_int, _i64, _vp, _vp, _i64p],
@@ -57,6 +58,7 @@ SIGNATURES = {
                                ctypes.POINTER(_vp), _i64p], ctypes.c_int),
     "fb_server_poll": ([_vp, _i64, _i64p, ctypes.POINTER(ctypes.c_double), _i64p], ctypes.c_int),
     "fb_server_wait": ([_vp], ctypes.c_int),
+    "fb_server_cancel": ([_vp, _i64], ctypes.c_int),
     "fb_server_stats": ([_vp, _i64p, ctypes.c_int], ctypes.c_int),
     "fb_server_reset_clock": ([_vp], ctypes.c_int),
     "fb_server_destroy": ([_vp], ctypes.c_int),

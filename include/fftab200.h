@@ -158,7 +158,11 @@ typedef struct fb_server_s* fb_server;
 int fb_server_create(fb_server* srv, double budget_bytes, int nstreams, uint32_t flags);
 /* Queue `batch` contiguous transforms of length n (device pointers; the
  * caller keeps them alive until the ticket completes).  Nothing is launched
- * until fb_server_poll / fb_server_wait. */
+ * until fb_server_poll / fb_server_wait.  A request whose device bytes
+ * (input, output and multi-pass scratch) exceed the whole budget is refused
+ * with FB_ERR_OUT_OF_MEMORY; a length the build has no schedule for with
+ * FB_ERR_UNSUPPORTED; n <= 0 with FB_ERR_DIMENSION_MISMATCH.  A refused
+ * request takes no ticket and leaves the queue as it was. */
 int fb_server_submit(fb_server srv, int64_t n, int dtype, int dir, int64_t batch, const void* in,
                      void* out, int64_t* ticket);
 /* fb_server_submit for `count` requests given as arrays (one call for every
@@ -170,11 +174,15 @@ int fb_server_submit_many(fb_server srv, int64_t count, const int64_t* n, const 
  * and return up to `max` completed tickets with their completion times (ms
  * on the device clock since fb_server_create). */
 int fb_server_poll(fb_server srv, int64_t max, int64_t* tickets, double* done_ms, int64_t* count);
+/* Withdraw a request that is still waiting (not yet dispatched): it never
+ * runs, its output is not written and poll never reports its ticket.
+ * FB_ERR_ARGUMENT if the ticket is unknown, already dispatched or done. */
+int fb_server_cancel(fb_server srv, int64_t ticket);
 /* Dispatch and wait until every submitted request has completed. */
 int fb_server_wait(fb_server srv);
-/* out[0..7]: requests, launches, descriptor launches, max queue depth, max
- * admitted bytes, resident plans, graph launches, graph captures (the first
- * `nout` of them). */
+/* out[0..8]: requests, launches, descriptor launches, max queue depth, max
+ * admitted bytes, resident plans, graph launches, graph captures, cancelled
+ * requests (the first `nout` of them). */
 int fb_server_stats(fb_server srv, int64_t* out, int nout);
 /* Restart the clock of fb_server_poll's completion times (waits until the
  * server's first stream is idle). */
@@ -204,8 +212,9 @@ int fb_plan_destroy(fb_plan plan);
  * array of 4,194,304 complex values (32 MiB, held by every GPU that loads the
  * library until exit) and its tables in a second static array.  Limits:
  * n*batch <= 4194304 (else FB_ERR_ARGUMENT) and n a product of 2s, 3s and 5s
- * (else FB_ERR_UNSUPPORTED).  All calls share the arrays: calls that overlap
- * on the GPU race.  The first call on a device looks up the arrays' addresses
+ * (else FB_ERR_UNSUPPORTED); batch < 0 gives FB_ERR_ARGUMENT.  `in` and
+ * `out` may be the same buffer.  All calls share the arrays: calls that
+ * overlap on the GPU race.  The first call on a device looks up the arrays' addresses
  * (make it before any stream capture).  Errors via fb_last_error(). */
 int fb_execute_noalloc_c32(const void* in, void* out, int64_t n, int64_t batch, int dir,
                            void* stream);
@@ -230,6 +239,17 @@ int fb_tune_cache_load(const char* path);
  * FFTA counterpart: FFTA raises ArgumentError("kernel not implemented")
  * for an unknown node type (src/algos.jl:31). */
 int fb_kernel_error_flag(int* value, int reset);
+
+/* Limit, in nanoseconds, of every wait a kernel makes on its own
+ * asynchronous work (the bulk copies of FB_FLAG_STREAM kernels, the products
+ * of FB_FLAG_TENSOR_STAGE kernels) for launches made after this call, in
+ * every thread of the process.  When a wait runs out the kernel sets the
+ * error flag to -1 (fb_kernel_error_flag), stops early and leaves its output
+ * partial; before it reuses or frees the memory those copies or products
+ * write, it still waits at least the default limit for them.  ns <= 0
+ * restores the default (about one second).  No FFTA counterpart: FFTA has no
+ * asynchronous work to wait for. */
+int fb_set_wait_limit(int64_t ns);
 
 /* Message of the last failing call on this thread ("" if none). */
 const char* fb_last_error(void);

@@ -334,6 +334,30 @@ def test_repeated_calls_reuse_the_checked_plan():
     assert len(p._fast) == 1
 
 
+def test_lazily_conjugated_and_negated_views():
+    """torch's conj() and -x of a view are flags, not storage: an input view
+    transforms its values, an output view receives them, and neither layout
+    enters the repeated-call shortcut."""
+    import torch
+    rng = np.random.default_rng(9)
+    xh = crandn(rng, (4, 1024), np.complex64)
+    x = torch.from_numpy(xh).cuda().T
+    p = F.plan_fft(x, 1)
+    for view, ref_in in ((x.conj(), np.conj(xh)), (torch._neg_view(x), -xh),
+                         (torch._neg_view(x.conj()), -np.conj(xh))):
+        assert view.is_conj() or view.is_neg()
+        for _ in range(2):  # the second call must not take a cached plan of the storage
+            y = (p * view).T.cpu().numpy()
+            ref = oracle.fft_batched(ref_in.astype(np.complex128), -1, nthreads=NTHR)
+            assert relerr(y, ref) <= tol(np.complex64, 1024)
+    out = torch.empty_like(x).conj()
+    for _ in range(2):
+        F.mul_(out, p, x)
+        ref = oracle.fft_batched(xh.astype(np.complex128), -1, nthreads=NTHR)
+        assert relerr(out.T.resolve_conj().cpu().numpy(), ref) <= tol(np.complex64, 1024)
+    torch.cuda.synchronize()
+
+
 def test_in_place_and_strided():
     import torch
     rng = np.random.default_rng(5)
@@ -405,19 +429,50 @@ def test_four_step_specialised_equals_generic(N, B, dtype):
         assert relerr(a, ref) <= tol(dtype, N)
 
 
-@pytest.mark.parametrize("N,B", [(1009, 64), (65537, 16), (1000003, 1), (2 ** 8 * 4099, 4)])
-def test_config3_bluestein_tone(N, B):
-    rng = np.random.default_rng(N)
-    x = crandn(rng, (B, N), np.complex64)
-    k0 = int(rng.integers(0, N))
-    tone = np.exp(2j * np.pi * k0 * np.arange(N) / N)
-    x = (x + tone * N).astype(np.complex64)  # unit tone, scaled above the noise floor
+CONFIG3 = [(1009, 64), (65537, 16), (1000003, 1), (2 ** 8 * 4099, 4)]
+
+
+def _blue_run(x, direction):
     import torch
     t = torch.from_numpy(x).cuda()
-    y = (F.plan_fft(np.asfortranarray(x.T), 1) * t.T).T.cpu().numpy()
+    planner = F.plan_fft if direction == -1 else F.plan_bfft
+    y = (planner(np.asfortranarray(x.T), 1) * t.T).T.cpu().numpy()
+    torch.cuda.synchronize()
+    return y
+
+
+@pytest.mark.parametrize("N,B", CONFIG3)
+def test_config3_bluestein_tone(N, B):
+    """Configuration 3 as stated: i.i.d. complex normal noise (sigma 1 per part)
+    plus a unit-amplitude tone at a seeded bin k0.  The tone's peak (N) must
+    land at k0 and the whole spectrum -- noise included, which carries almost
+    all of the norm here -- must match the FP64 oracle."""
+    rng = np.random.default_rng(N)
+    x = crandn(rng, (B, N))
+    k0 = int(rng.integers(0, N))
+    x = (x + np.exp(2j * np.pi * k0 * np.arange(N) / N)).astype(np.complex64)
+    y = _blue_run(x, -1)
     ref = oracle.fft_batched(x.astype(np.complex128), -1, nthreads=NTHR)
     assert relerr(y, ref) <= tol(np.complex64, N)
     assert np.all(np.argmax(np.abs(y), axis=1) == k0)
+
+
+@pytest.mark.parametrize("direction", [-1, 1])
+@pytest.mark.parametrize("N,B", CONFIG3)
+def test_config3_bluestein_noise(N, B, direction):
+    """Noise only, both directions, at the configuration-3 lengths (BLUE1 for
+    1009; three-pass Bluestein for 65537 and 1000003, whose pads above 2^18
+    take their twiddles from root tables on the passes' stores; a four-step
+    split with a Bluestein pass for 2^8 * 4099).  rel-L2 against the FP64
+    oracle within 4 eps(Float32) log2 N, and per transform as well, so no
+    column can hide behind the others."""
+    rng = np.random.default_rng(N + 7 * direction)
+    x = crandn(rng, (B, N), np.complex64)
+    y = _blue_run(x, direction)
+    ref = oracle.fft_batched(x.astype(np.complex128), direction, nthreads=NTHR)
+    assert relerr(y, ref) <= tol(np.complex64, N)
+    for b in range(B):
+        assert relerr(y[b], ref[b]) <= tol(np.complex64, N), b
 
 
 @pytest.mark.parametrize("m,n", [(4096, 4096), (2187, 2048), (1000, 1000)])

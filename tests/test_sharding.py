@@ -59,3 +59,44 @@ def test_two_rank_gloo():
 def test_no_group_is_identity():
     assert sharding.max_over_ranks(3.0) == 3.0
     assert sharding.whole_job_rate(10, 2.0) == 5.0
+
+
+def _bench():
+    import importlib.util
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(root, "bench.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_bench_starts_its_own_ranks(tmp_path, monkeypatch):
+    """`bench.py --gpus N` without torchrun re-runs itself under
+    torch.distributed.run with N ranks; inside a rank (WORLD_SIZE set) or for
+    N = 1 it runs in place.  The command is run here for real on a stand-in
+    script whose two ranks meet over gloo."""
+    import subprocess
+    import sys
+    bench = _bench()
+    monkeypatch.delenv("WORLD_SIZE", raising=False)
+    cmd = bench.launch_command(4, ["--gpus", "4", "--steps", "3"], port=29123)
+    assert cmd[:3] == [sys.executable, "-m", "torch.distributed.run"]
+    assert "--nproc-per-node=4" in cmd and cmd[cmd.index("--master-addr") + 1] == "127.0.0.1"
+    assert cmd[-4:] == ["--gpus", "4", "--steps", "3"] and cmd[-5].endswith("bench.py")
+    assert bench.maybe_launch(1, []) is None
+    monkeypatch.setenv("WORLD_SIZE", "2")
+    assert bench.maybe_launch(2, []) is None
+    monkeypatch.delenv("WORLD_SIZE")
+    script = tmp_path / "rank.py"
+    script.write_text(
+        "import os, datetime, torch, torch.distributed as dist\n"
+        "dist.init_process_group('gloo', timeout=datetime.timedelta(seconds=60))\n"
+        "t = torch.tensor([float(os.environ['RANK']) + 1])\n"
+        "dist.all_reduce(t)\n"
+        "os.write(1, f\"sum={int(t.item())}:{os.environ['WORLD_SIZE']}\\n\".encode())\n"
+        "dist.destroy_process_group()\n")
+    out = subprocess.run(bench.launch_command(2, [], port=29000 + os.getpid() % 500,
+                                              script=str(script)),
+                         capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert out.stdout.count("sum=3:2") == 2, out.stdout
