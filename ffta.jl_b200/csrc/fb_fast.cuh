@@ -440,12 +440,13 @@ __global__ void __launch_bounds__(T, StreamBounds<R, RL, T>::min_blocks)
   for (; i < nmine; ++i) {
     const int b = (int)(i % NBUF);
     const bool got = mbar_wait(bar + b, (uint32_t)((i / NBUF) & 1), a.wait_ns);
-    // every thread has also finished line i-1, so its buffer is free
+    // this thread's writes to line i-1's buffer are ordered before the copy
+    // that refills it, and every thread has finished line i-1
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (!__syncthreads_and(got)) break;
     const int64_t nx = i + NBUF - 1;
     if (u == 0 && nx < nmine) {
       const int bb = (int)(nx % NBUF);
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_expect_tx(bar + bb, SS::bytes);
       bulk_load(buffer(bb), gin + (first + nx * step) * a.idist, SS::bytes, bar + bb);
     }
@@ -587,6 +588,123 @@ __global__ void __launch_bounds__(TileThreads<R, T, MID>::value,
       else
         fast_prog<R, 1, RL, T>(buf, in, out, tw, pcs, u);
     }
+  }
+}
+
+// ------------------------------------------------------ TMA tile kernel
+// The lean tile kernel for passes whose lines are neighbours in memory
+// (four-step columns, strided 2-D axes): instead of each thread loading its
+// butterfly's inputs from HBM (short strided segments whose latency the
+// block then waits out), one thread issues tensor copies
+// (cp.async.bulk.tensor) of whole tiles -- G neighbouring lines x L elements
+// -- into shared memory, `nbuf` tiles ahead, each completing on an mbarrier.
+// Blocks are persistent: block b transforms tiles b, b + gridDim.x, ...  So
+// HBM keeps streaming the next tiles while the block computes this one.
+// The first stage reads the landed tile (element i of line g at t[i*G + g]),
+// then every stage runs as in fast_tile_kernel, in the same buffer, and the
+// last stage stores to HBM from registers; the arithmetic is the same, so
+// results equal the other kernels' bit for bit.  Tensor maps cover this GPU's
+// own memory only and no copy is multicast.  Every wait is bounded: a block
+// that gives up sets kErrWaitTimeout, drains its copies in flight (at least
+// the default limit) and returns.
+
+// One box of a 4-D tensor map (x: lines in 8-byte units, y: elements of the
+// line, z/w: batch levels) into shared memory, completing on *bar.
+__device__ __forceinline__ void tma_load_4d(void* dst, const void* tmap, int x, int y, int z,
+                                            int w, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(z), "r"(w),
+      "r"(smem_addr(bar))
+      : "memory");
+}
+
+// Element i of line g read from a landed tile (this thread's line: t + g,
+// stride G); the four-step twiddle on the loads as PlainIn applies it.
+template <typename R> struct TmaIn : PlainIn<R> {
+  __device__ __forceinline__ cplx<R> raw(int i) const { return this->base[i * this->es]; }
+};
+template <typename R> struct InHasBfly<TmaIn<R>> : std::true_type {};
+template <typename R> struct InIsSmem<TmaIn<R>> : std::true_type {};
+
+template <typename R, class RL, int T>
+__global__ void __launch_bounds__(TileThreads<R, T, false>::value,
+                                  TileBounds<R, RL, T, false, true>::min_blocks)
+    fast_tma_tile_kernel(const LineArgs a, const __grid_constant__ CUtensorMap tm,
+                         const TmaGeom q) {
+  typedef cplx<R> C;
+  constexpr int L = prog_len<RL>();
+  constexpr int LPAD = lpad_of(L);
+  // the buffers start 128-byte aligned (tensor copies land there); the
+  // launch reserves 128 bytes for the adjustment
+  extern __shared__ __align__(16) unsigned char smtma[];
+  unsigned char* smraw = smtma + ((128u - (smem_addr(smtma) & 127u)) & 127u);
+  const int g = threadIdx.x, u = threadIdx.y, G = a.G;
+  const int tid = g + G * u;
+  const int P = tile_pitch(LPAD, G, (int)sizeof(C));
+  uint64_t* bar = (uint64_t*)(smraw + (size_t)q.nbuf * q.buf_bytes);
+  const int64_t first = blockIdx.x, step = gridDim.x;
+  const int64_t nmine = first < q.ntiles ? (q.ntiles - 1 - first) / step + 1 : 0;
+  const uint32_t tile_bytes = (uint32_t)(L * G * (int)sizeof(C));
+  const uint32_t box_bytes = (uint32_t)(q.boxr * G * (int)sizeof(C));
+  // the copies of this block's k-th tile into buffer b (thread 0 only)
+  auto issue = [&](int64_t k, int b) {
+    const int64_t line = (first + k * step) * G;
+    const int64_t q0 = line % a.m0, t = line / a.m0;
+    const int64_t q1 = t % a.m1, q2 = t / a.m1;
+    unsigned char* dst = smraw + (size_t)b * q.buf_bytes;
+    mbar_expect_tx(bar + b, tile_bytes);
+    for (int r = 0; r < q.nbox; ++r)
+      tma_load_4d(dst + (size_t)r * box_bytes, &tm, (int)(q0 * q.units), r * q.boxr, (int)q1,
+                  (int)q2, bar + b);
+  };
+  if (tid == 0) {
+    for (int b = 0; b < q.nbuf; ++b) mbar_init(bar + b, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int b = 0; b < q.nbuf - 1 && b < nmine; ++b) issue(b, b);
+  }
+  __syncthreads();
+  const C* tw = (const C*)a.prog.tw;
+  const R* pcs = (const R*)a.prime_cs;
+  const C* tin = a.tw_on_load ? (const C*)a.tw_tab : nullptr;
+  const C* tout = a.tw_on_load ? nullptr : (const C*)a.tw_tab;
+  int64_t k = 0;
+  for (; k < nmine; ++k) {
+    const int b = (int)(k % q.nbuf);
+    const bool got = mbar_wait(bar + b, (uint32_t)((k / q.nbuf) & 1), a.wait_ns);
+    // this thread's writes to tile k-1's buffer (its stage exchanges) are
+    // ordered before the tensor copy that refills it ...
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    // ... and every thread has finished tile k-1
+    if (!__syncthreads_and(got)) break;
+    const int64_t nx = k + q.nbuf - 1;
+    if (tid == 0 && nx < nmine) issue(nx, (int)(nx % q.nbuf));
+    const int64_t line = (first + k * step) * G + g;
+    const int64_t q0 = line % a.m0, t = line / a.m0;
+    const int64_t q1 = t % a.m1, q2 = t / a.m1;
+    const int64_t lt = a.tw_level ? q1 : q0;
+    C* tile = (C*)(smraw + (size_t)b * q.buf_bytes);
+    TmaIn<R> in;
+    in.base = tile + g;
+    in.es = G;
+    in.tab = tin;
+    in.tab_es = (int)a.tw_es;
+    in.tab_off = (int)(lt * a.tw_ls);
+    in.tw_dir = a.tw_dir;
+    const PlainOut<R> out{(C*)a.out + q0 * a.st.s0 + q1 * a.st.s1 + q2 * a.st.s2, (int)a.st.es,
+                          tout, (int)a.tw_es, (int)(lt * a.tw_ls), a.tw_dir, (R)a.scale, true,
+                          a.st_stream != 0};
+    if (a.dir1 < 0)
+      fast_prog<R, -1, RL, T>(tile + g * P, in, out, tw, pcs, u);
+    else
+      fast_prog<R, 1, RL, T>(tile + g * P, in, out, tw, pcs, u);
+  }
+  if (k < nmine && tid == 0) {
+    // gave up on tile k: flag it, then let the copies still in flight land
+    if (a.err) atomicExch(a.err, kErrWaitTimeout);
+    for (int64_t j = k; j < nmine && j < k + q.nbuf - 1; ++j)
+      mbar_wait(bar + (int)(j % q.nbuf), (uint32_t)((j / q.nbuf) & 1), drain_limit(a.wait_ns));
   }
 }
 
@@ -782,6 +900,43 @@ template <typename R, class RL, int T> struct FastEntry {
       k<<<dim3((unsigned)nblk), dim3(T), smem, s>>>(a);
       e = cudaGetLastError();
       if (e != cudaSuccess) launch_failure(k, "stream launch", L, T, 1, smem, e);
+      return e;
+    }
+  }
+  // Tensor-copy tile kernel: lengths 8..4096 (longer lines leave no room for
+  // a second tile buffer).  As many persistent blocks as fit at once, at most
+  // one per tile.
+  static constexpr bool has_tma = L >= 8 && L <= 4096;
+  static cudaError_t launch_tile_tma(const LineArgs& a, const void* tmap, const TmaGeom& q,
+                                     cudaStream_t s) {
+    if constexpr (!has_tma) {
+      snprintf(g_launch_msg, sizeof(g_launch_msg), "no tensor-copy tile kernel for L=%d", L);
+      return cudaErrorNotSupported;
+    } else {
+      static int set[64] = {0};
+      const size_t smem = (size_t)q.nbuf * q.buf_bytes + 64 + 128;
+      auto k = fast_tma_tile_kernel<R, RL, T>;
+      if (a.G * T > TILE_THREADS || a.mid || !a.plain_io || q.nbuf < 2) {
+        launch_failure(k, "tensor-copy tile shape", L, T, a.G, smem, cudaErrorInvalidValue);
+        return cudaErrorInvalidValue;
+      }
+      int dev = 0, per_sm = 0, nsm = 0;
+      cudaError_t e = cudaGetDevice(&dev);
+      if (e == cudaSuccess) e = configure(k, smem, set);
+      if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, a.G * T, smem);
+      if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      if (e == cudaSuccess && per_sm < 1) e = cudaErrorInvalidConfiguration;
+      if (e != cudaSuccess) {
+        launch_failure(k, "tensor-copy tile set-up", L, T, a.G, smem, e);
+        return e;
+      }
+      if (q.ntiles <= 0) return cudaSuccess;
+      const int64_t cap = (int64_t)per_sm * nsm;
+      const int64_t nblk = q.ntiles < cap ? q.ntiles : cap;
+      k<<<dim3((unsigned)nblk), dim3(a.G, T), smem, s>>>(a, *(const CUtensorMap*)tmap, q);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) launch_failure(k, "tensor-copy tile launch", L, T, a.G, smem, e);
       return e;
     }
   }

@@ -26,7 +26,10 @@ namespace fb {
    FastEntry<FB_R, RList<__VA_ARGS__>, T>::has_tile_tc                         \
        ? &FastEntry<FB_R, RList<__VA_ARGS__>, T>::launch_tile_tc               \
        : nullptr,                                                              \
-   FastEntry<FB_R, RList<__VA_ARGS__>, T>::TILE_THREADS}
+   FastEntry<FB_R, RList<__VA_ARGS__>, T>::TILE_THREADS,                      \
+   FastEntry<FB_R, RList<__VA_ARGS__>, T>::has_tma                             \
+       ? &FastEntry<FB_R, RList<__VA_ARGS__>, T>::launch_tile_tma              \
+       : nullptr}
 
 static const FastFn kTable[] = {
 #include "fb_fast_table.inc"

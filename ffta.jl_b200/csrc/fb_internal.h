@@ -1,6 +1,7 @@
 // fb_internal.h -- structures shared by the planner (fb_plan.cu) and the
 // kernels (fb_kernels.cu).  Not part of the public C ABI.
 #pragma once
+#include <cuda.h>  // CUtensorMap (types only; the driver is reached through cudart)
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -124,6 +125,18 @@ constexpr uint64_t kWaitNsDefault = 1000000000ull;
 // The limit a launch uses: fb_set_wait_limit's value, 0 for the default.
 uint64_t wait_limit_ns();
 
+// Geometry of a tile pass whose loads are tensor copies (fast_tma_tile_kernel):
+// tile k holds lines k*G .. k*G+G-1 (G divides the first batch level, so a
+// tile's lines are neighbours in memory), brought into shared memory as
+// `nbox` boxes of `boxr` elements x G lines.
+struct TmaGeom {
+  int nbox, boxr;      // boxes per tile along the line, elements per box
+  int units;           // 8-byte units per element (1: ComplexF32, 2: ComplexF64)
+  int nbuf;            // tile buffers in flight per block
+  uint32_t buf_bytes;  // bytes per buffer (flat tile or padded lines; 1 KB multiple)
+  int64_t ntiles;
+};
+
 // One specialised length: its radix program, threads per line, launcher and
 // padded shared-memory elements per line.
 struct FastFn {
@@ -141,6 +154,10 @@ struct FastFn {
   cudaError_t (*launch_tile_tc)(const LineArgs&, cudaStream_t);
   // threads per block of launch_tile outside Bluestein (G * T at most)
   int tile_threads;
+  // the lean tile kernel fed by tensor copies (persistent blocks, `nbuf`
+  // tiles in flight); `tmap` is the CUtensorMap of the pass's input;
+  // nullptr where the length has none
+  cudaError_t (*launch_tile_tma)(const LineArgs&, const void* tmap, const TmaGeom&, cudaStream_t);
 };
 
 // Bytes of one direction's B table of the tensor-core radix-16 stage.
@@ -185,6 +202,30 @@ cudaError_t gen_chirp(int dtype, void* pre, void* post, void* bext_c64, int64_t 
 cudaError_t convert_c64(int dtype, void* dst, const void* src_c64, int64_t n, double scale,
                         cudaStream_t s);
 cudaError_t gen_prime_tables(void* f32tab, void* f64tab, cudaStream_t s);
+
+// The serving loop's resident kernel and its descriptor queue (fb_serve.cu).
+struct PQueue;
+enum { kPqStatOk = 0, kPqStatTimeout = 1, kPqStatBadProgram = 2 };
+// Program id of contiguous lines of length L (16..4096, powers of two), or -1.
+int pq_program_id(int dtype, int dir, int64_t L);
+// Queue with its buffers; the kernel ends after `idle_ns` without new work.
+cudaError_t pq_create(PQueue** q, uint64_t idle_ns);
+void pq_destroy(PQueue* q);
+// Register program `id` with its stage twiddle table and odd-prime table.
+cudaError_t pq_set_program(PQueue* q, int id, const void* tw, const void* pcs);
+bool pq_has_program(const PQueue* q, int id);
+int64_t pq_slots();
+// Append a request (returns its queue index); pq_publish makes the appended
+// ones visible to the kernel; pq_kick launches the kernel if none is resident.
+int64_t pq_push(PQueue* q, int prog, const void* in, void* out, int64_t batch, int64_t seq_add);
+void pq_publish(PQueue* q);
+cudaError_t pq_kick(PQueue* q);
+bool pq_running(PQueue* q);
+// 1 when request r has completed (time in globaltimer ns, status kPqStat*).
+int pq_poll(PQueue* q, int64_t r, int64_t* t_ns, int32_t* status);
+// The device globaltimer, read by a one-thread kernel on `s` into mapped
+// host memory (device and host addresses of one int64).
+cudaError_t pq_clock(cudaStream_t s, int64_t* host_mapped_dev, int64_t* host_mapped);
 
 // Real-transform helpers on contiguous column-major arrays (dtype 0: float /
 // ComplexF32, 1: double / ComplexF64).

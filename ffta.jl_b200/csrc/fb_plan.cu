@@ -20,7 +20,9 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
+#include <thread>
 #include <cstdio>
 #include <cstring>
 #include <functional>
@@ -96,7 +98,10 @@ static const DeviceTables& device_tables(int dev) {
   cuda_check(cudaMalloc(&t.err, sizeof(int)), "cudaMalloc");
   cuda_check(cudaMemset(t.err, 0, sizeof(int)), "cudaMemset");
   cuda_check(gen_prime_tables(t.f32, t.f64, 0), "prime tables");
-  cuda_check(cudaDeviceSynchronize(), "prime tables");
+  // table work runs on the legacy default stream; waiting for it alone (not
+  // the whole device) keeps plan creation independent of a serving loop's
+  // resident kernel on its non-blocking stream
+  cuda_check(cudaStreamSynchronize(0), "prime tables");
   return g_dev_tables.emplace(dev, t).first->second;
 }
 
@@ -381,6 +386,12 @@ struct Pass {
   const FastFn* staged = nullptr;  // specialised tile kernel (strided lines, fused I/O)
   int stream = 0;                  // 1: run `fast` as its persistent bulk-copy kernel
   int tc = 0;                      // 1: first radix-16 stage on the tensor cores
+  int tma = 0;                     // 1: run `staged` fed by tensor copies (geometry tg)
+  TmaGeom tg;
+  // the tensor map of the last input this pass ran on (re-encoded when the
+  // input address changes)
+  CUtensorMap tmap;
+  const void* tmap_in = nullptr;
 };
 
 // The specialised kernel for a radix program, if one is compiled.
@@ -458,6 +469,8 @@ namespace fb {
 
 static int pick_G(const fb_plan_s* P, int L, int T, int Lpad, bool elem_major, int64_t nlines);
 static void apply_tuning(fb_plan_s* P);
+static void plan_tma(const fb_plan_s* P, Pass& p);
+static int lpad_for(int L);
 
 // Lines per block of the tile kernel: by its threads (FastFn::tile_threads),
 // and by shared memory -- 100 KB for ComplexF32 (two blocks per SM), up to
@@ -525,6 +538,107 @@ static void use_tile(const fb_plan_s* P, Pass& p, const std::vector<int>& radice
     p.a.tcb = tc_tables(P->device);
   }
   p.what += "[tile T=" + std::to_string(T) + " G=" + std::to_string(p.a.G) + "]";
+  plan_tma(P, p);
+}
+
+// Tensor-copy geometry of a lean tile pass with G lines per tile, or false
+// when the pass cannot take tensor copies: its lines must be neighbours in
+// memory (element-major loads, line stride 1) and G must divide the first
+// batch level (a tile never straddles it), the rows of a box must cover
+// whole 32-byte sectors and 16-byte units, and two tiles must fit in shared
+// memory.  Shared memory per block: up to ~110 KB (two blocks per SM) when
+// two or three buffers fit there, else up to ~220 KB (one block per SM).
+static bool tma_geometry(const fb_plan_s* P, const Pass& p, int G, TmaGeom* g) {
+  const FastFn* ff = p.staged;
+  const LineArgs& a = p.a;
+  if (!ff || !ff->launch_tile_tma || p.tc || !a.plain_io || a.mid) return false;
+  if (a.ld.mode != 1 || a.ld.s0 != 1 || G < 2 || G * ff->T > ff->tile_threads) return false;
+  const int es = elem_bytes(P->dtype);
+  const int L = a.prog.L;
+  if (a.m0 % G || a.nlines % G || G * es < 32) return false;
+  const int64_t m2 = a.nlines / std::max<int64_t>(1, a.m0 * a.m1);
+  if (a.m0 * a.m1 * m2 != a.nlines) return false;
+  for (int64_t st : {a.ld.es, a.ld.s1, a.ld.s2})
+    if ((st * es) % 16 || std::llabs(st) * es >= (int64_t(1) << 39)) return false;
+  if (a.m0 * (es / 8) >= (int64_t(1) << 31) || a.m1 >= (int64_t(1) << 31) || m2 >= (int64_t(1) << 31))
+    return false;
+  // boxes of at most 256 elements that split the line evenly, each landing
+  // 128-byte aligned
+  int nbox = (L + 255) / 256;
+  while (nbox <= L && (L % nbox || ((size_t)(L / nbox) * G * es) % 128)) ++nbox;
+  if (nbox > L || nbox > 64) return false;
+  const int boxr = L / nbox;
+  const size_t flat = (size_t)L * G * es;
+  const size_t padded = (size_t)G * tile_pitch(lpad_for(L), G, es) * es;
+  const size_t buf = (std::max(flat, padded) + 1023) / 1024 * 1024;
+  int nbuf = (int)std::min<size_t>(3, (110 * 1024) / buf);
+  if (nbuf < 2) nbuf = (int)std::min<size_t>(3, (220 * 1024) / buf);
+  if (nbuf < 2) return false;
+  g->nbox = nbox;
+  g->boxr = boxr;
+  g->units = es / 8;
+  g->nbuf = nbuf;
+  g->buf_bytes = (uint32_t)buf;
+  g->ntiles = a.nlines / G;
+  return true;
+}
+
+// Switch a lean tile pass to tensor-copy loads where it qualifies, with as
+// many lines per tile as give 128-byte rows (64 at least) within the block's
+// thread limit.
+static void plan_tma(const fb_plan_s* P, Pass& p) {
+  if ((P->flags & FB_FLAG_NO_TMA) || !p.staged) return;
+  const int es = elem_bytes(P->dtype);
+  for (int G = 128 / es; G * es >= 32; G /= 2) {
+    TmaGeom g;
+    if (!tma_geometry(P, p, G, &g)) continue;
+    p.tma = 1;
+    p.tg = g;
+    p.a.G = G;
+    p.what += "<tma G=" + std::to_string(G) + " bufs=" + std::to_string(g.nbuf) + ">";
+    return;
+  }
+}
+
+// CUtensorMap of a tensor-copy pass over the input `in` (4-D: lines in
+// 8-byte units, elements, the two batch levels).
+static bool encode_tma(const fb_plan_s* P, Pass& p, const void* in) {
+  typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                               const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                               const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                               CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static EncodeFn encode = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult qr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &qr) ==
+            cudaSuccess &&
+        qr == cudaDriverEntryPointSuccess)
+      encode = (EncodeFn)fn;
+    cudaGetLastError();
+  });
+  if (!encode || reinterpret_cast<uintptr_t>(in) % 16) return false;
+  if (p.tmap_in == in) return true;
+  const LineArgs& a = p.a;
+  const int es = elem_bytes(P->dtype);
+  const int64_t m2 = a.nlines / (a.m0 * a.m1);
+  const cuuint64_t row = (cuuint64_t)(a.ld.es * es);
+  const cuuint64_t dims[4] = {(cuuint64_t)(a.m0 * (es / 8)), (cuuint64_t)a.prog.L,
+                              (cuuint64_t)a.m1, (cuuint64_t)m2};
+  // strides of extent-1 levels are never used; give them a valid value
+  const cuuint64_t s1 = a.m1 > 1 ? (cuuint64_t)(a.ld.s1 * es) : row * a.prog.L;
+  const cuuint64_t s2 = m2 > 1 ? (cuuint64_t)(a.ld.s2 * es) : s1 * a.m1;
+  const cuuint64_t strides[3] = {row, s1, s2};
+  const cuuint32_t box[4] = {(cuuint32_t)(a.G * (es / 8)), (cuuint32_t)p.tg.boxr, 1, 1};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  const CUresult r =
+      encode(&p.tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<void*>(in), dims, strides,
+             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return false;
+  p.tmap_in = in;
+  return true;
 }
 
 static void* alloc_table(fb_plan_s* P, size_t bytes) {
@@ -583,7 +697,7 @@ static void* chirp_spectrum(fb_plan_s* P, int64_t N, int64_t M, double scale) {
   execute_plan(sub.get(), bext.p, spec.p, 0);
   void* mid = alloc_table(P, (size_t)M * elem_bytes(P->dtype));
   cuda_check(convert_c64(P->dtype, mid, spec.p, M, scale, 0), "chirp spectrum");
-  cuda_check(cudaDeviceSynchronize(), "chirp spectrum");
+  cuda_check(cudaStreamSynchronize(0), "chirp spectrum");
   return mid;
 }
 
@@ -1244,7 +1358,7 @@ static fb_plan_s* create_plan(int dtype, int dir, int rank, const int64_t* dims,
       for (auto& p : ax.passes) need1 |= p.src == B_S1 || p.dst == B_S1;
     if (need1) P->scratch1.reset(new DevBuf(P->scratch_elems * elem_bytes(dtype)));
   }
-  cuda_check(cudaDeviceSynchronize(), "plan tables");
+  cuda_check(cudaStreamSynchronize(0), "plan tables");
   apply_tuning(P.get());
   return P.release();
 }
@@ -1309,6 +1423,14 @@ static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s
         }
         if (last && P->scale != 1.0) a.scale = P->scale * a.scale;
         if (p.staged) {
+          // tensor copies need the geometry for the current lines per tile
+          // (the autotuner may have changed them) and a 16-byte aligned input
+          TmaGeom tg;
+          if (p.tma && tma_geometry(P, p, a.G, &tg) && encode_tma(P, p, a.in)) {
+            const cudaError_t e = p.staged->launch_tile_tma(a, &p.tmap, tg, s);
+            if (e != cudaSuccess) cuda_check(e, last_launch_message());
+            continue;
+          }
           const cudaError_t e = p.tc ? p.staged->launch_tile_tc(a, s) : p.staged->launch_tile(a, s);
           if (e != cudaSuccess) cuda_check(e, last_launch_message());
           continue;
@@ -1768,7 +1890,22 @@ struct fb_server_s {
   std::vector<std::pair<cudaEvent_t, cudaGraphExec_t>> graph_retiring;
   int64_t graph_clock = 0, st_graph_launches = 0, st_graph_captures = 0;
   int64_t st_launches = 0, st_desc_launches = 0, st_requests = 0, st_max_queue = 0;
-  int64_t st_cancelled = 0;
+  int64_t st_cancelled = 0, st_resident = 0, st_failed = 0;
+  // the resident kernel's descriptor queue (small requests of served
+  // lengths), its outstanding requests, and the device clock origin
+  struct PqDeleter {
+    void operator()(fb::PQueue* q) const { fb::pq_destroy(q); }
+  };
+  std::unique_ptr<fb::PQueue, PqDeleter> pq;
+  struct PqReq {
+    int64_t r, ticket;
+    double bytes;
+  };
+  std::vector<PqReq> pq_out;
+  int64_t* clk_host = nullptr;  // mapped pinned: globaltimer at the clock origin
+  int64_t* clk_dev = nullptr;
+  int64_t clk0_ns = 0;
+  int64_t pq_seq_add = 0;  // fault injection (tests): next descriptor never arrives
   double st_max_admitted = 0;
   ~fb_server_s() {
     for (auto& g : graph_of) cudaGraphExecDestroy(g.second.exec);
@@ -1781,6 +1918,8 @@ struct fb_server_s {
       if (sl.last) cudaEventDestroy(sl.last);
       if (sl.host) cudaFreeHost(sl.host);
     }
+    pq.reset();
+    if (clk_host) cudaFreeHost(clk_host);
     for (auto s : streams) cudaStreamDestroy(s);
     for (auto s : multi_streams) cudaStreamDestroy(s);
     if (start) cudaEventDestroy(start);
@@ -1900,8 +2039,32 @@ static void srv_run_plan(fb_server_s* S, fb_plan_s* P, const void* in, void* out
   S->st_graph_launches += 1;
 }
 
+// Completed requests of the resident kernel's queue; relaunches the kernel
+// while requests are outstanding and none is resident (it ends when idle).
+// Completion times come from the device globaltimer; a request the kernel
+// gave up on (kPqStat*) completes with time -1.
+static void srv_reap_resident(fb_server_s* S) {
+  if (S->pq_out.empty()) return;
+  size_t keep = 0;
+  for (size_t i = 0; i < S->pq_out.size(); ++i) {
+    const auto& q = S->pq_out[i];
+    int64_t t = 0;
+    int32_t st = 0;
+    if (pq_poll(S->pq.get(), q.r, &t, &st)) {
+      S->done.push_back({q.ticket, st == kPqStatOk ? (double)(t - S->clk0_ns) * 1e-6 : -1.0});
+      if (st != kPqStatOk) S->st_failed += 1;
+      S->admitted -= q.bytes;
+    } else {
+      S->pq_out[keep++] = q;
+    }
+  }
+  S->pq_out.resize(keep);
+  if (!S->pq_out.empty()) cuda_check(pq_kick(S->pq.get()), "resident kernel launch");
+}
+
 static void srv_retire(fb_server_s* S, bool block) {
   if (!S->graph_retiring.empty()) srv_sweep_graphs(S);
+  srv_reap_resident(S);
   while (!S->inflight.empty()) {
     bool done_any = false;
     for (auto it = S->inflight.begin(); it != S->inflight.end();) {
@@ -1977,7 +2140,23 @@ static void srv_dispatch(fb_server_s* S) {
     size_t smem = 0;
   };
   std::map<std::tuple<int, int, int, int>, Group> groups;
+  bool resident = false;
   for (const SrvReq& r : batch) {
+    // small requests of a served length go to the resident kernel's queue
+    const int pid = r.shape && S->pq ? pq_program_id(r.dtype, r.dir, r.n) : -1;
+    if (pid >= 0 && (int64_t)S->pq_out.size() < pq_slots() - 1) {
+      if (!pq_has_program(S->pq.get(), pid)) {
+        const Pass& tp = srv_template(S, r.n, r.dtype, r.dir)->axes[0].passes[0];
+        cuda_check(pq_set_program(S->pq.get(), pid, tp.a.prog.tw, tp.a.prime_cs),
+                   "resident program table");
+      }
+      const int64_t q = pq_push(S->pq.get(), pid, r.in, r.out, r.batch, S->pq_seq_add);
+      S->pq_seq_add = 0;
+      S->pq_out.push_back({q, r.ticket, r.bytes});
+      S->st_resident += 1;
+      resident = true;
+      continue;
+    }
     if (!r.shape) {
       fb_plan_s* P = srv_multi(S, r.n, r.dtype, r.dir, r.batch);
       auto ms = S->multi_stream_of.find(P);
@@ -2015,6 +2194,10 @@ static void srv_dispatch(fb_server_s* S) {
     g.tickets.push_back(r.ticket);
     g.bytes += r.bytes;
     g.smem = std::max(g.smem, line_smem_bytes(r.dtype, sh.a));
+  }
+  if (resident) {
+    pq_publish(S->pq.get());
+    cuda_check(pq_kick(S->pq.get()), "resident kernel launch");
   }
   for (auto& kv : groups) {
     Group& g = kv.second;
@@ -2103,6 +2286,16 @@ int fb_server_create(fb_server* srv, double budget_bytes, int nstreams, uint32_t
     cuda_check(cudaEventCreate(&S->start), "event");
     cuda_check(cudaEventRecord(S->start, S->streams[0]), "event record");
     cuda_check(cudaEventSynchronize(S->start), "event sync");
+    if (!(flags & FB_SERVER_NO_PERSISTENT)) {
+      PQueue* q = nullptr;
+      cuda_check(pq_create(&q, 2000000), "persistent queue");  // ends after 2 ms idle
+      S->pq.reset(q);
+      cuda_check(cudaHostAlloc((void**)&S->clk_host, sizeof(int64_t), cudaHostAllocMapped),
+                 "clock");
+      cuda_check(cudaHostGetDevicePointer((void**)&S->clk_dev, S->clk_host, 0), "clock");
+      cuda_check(pq_clock(S->streams[0], S->clk_dev, S->clk_host), "clock");
+      S->clk0_ns = *(volatile int64_t*)S->clk_host;
+    }
     *srv = S.release();
   });
 }
@@ -2170,6 +2363,14 @@ int fb_server_poll(fb_server srv, int64_t max, int64_t* tickets, double* done_ms
   });
 }
 
+int fb_server_drop_next_descriptor(fb_server srv) {
+  return guard([&] {
+    if (!srv) fail(FB_ERR_ARGUMENT, "null argument");
+    if (!srv->pq) fail(FB_ERR_UNSUPPORTED, "the server has no resident kernel");
+    srv->pq_seq_add = int64_t(1) << 41;  // a sequence number no request ever has
+  });
+}
+
 int fb_server_cancel(fb_server srv, int64_t ticket) {
   return guard([&] {
     if (!srv) fail(FB_ERR_ARGUMENT, "null argument");
@@ -2187,9 +2388,22 @@ int fb_server_cancel(fb_server srv, int64_t ticket) {
 int fb_server_wait(fb_server srv) {
   return guard([&] {
     if (!srv) fail(FB_ERR_ARGUMENT, "null argument");
-    while (!srv->pending.empty() || !srv->inflight.empty()) {
+    // requests of the resident kernel complete in host memory: poll them,
+    // giving up (an error) after 30 s without any completing
+    auto last = std::chrono::steady_clock::now();
+    size_t outstanding = (size_t)-1;
+    while (!srv->pending.empty() || !srv->inflight.empty() || !srv->pq_out.empty()) {
       srv_dispatch(srv);
-      srv_retire(srv, true);
+      srv_retire(srv, srv->pq_out.empty());
+      if (srv->pq_out.empty()) continue;
+      const size_t n = srv->pq_out.size() + srv->pending.size() + srv->inflight.size();
+      if (n != outstanding) {
+        outstanding = n;
+        last = std::chrono::steady_clock::now();
+      } else if (std::chrono::steady_clock::now() - last > std::chrono::seconds(30)) {
+        fail(FB_ERR_CUDA, "resident kernel made no progress for 30 s");
+      }
+      std::this_thread::yield();
     }
   });
 }
@@ -2197,11 +2411,12 @@ int fb_server_wait(fb_server srv) {
 int fb_server_stats(fb_server srv, int64_t* out, int nout) {
   return guard([&] {
     if (!srv || !out) fail(FB_ERR_ARGUMENT, "null argument");
-    const int64_t v[9] = {srv->st_requests, srv->st_launches, srv->st_desc_launches,
-                          srv->st_max_queue, (int64_t)srv->st_max_admitted,
-                          (int64_t)(srv->templ.size() + srv->multi.size()),
-                          srv->st_graph_launches, srv->st_graph_captures, srv->st_cancelled};
-    for (int i = 0; i < nout && i < 9; ++i) out[i] = v[i];
+    const int64_t v[11] = {srv->st_requests, srv->st_launches, srv->st_desc_launches,
+                           srv->st_max_queue, (int64_t)srv->st_max_admitted,
+                           (int64_t)(srv->templ.size() + srv->multi.size()),
+                           srv->st_graph_launches, srv->st_graph_captures, srv->st_cancelled,
+                           srv->st_resident, srv->st_failed};
+    for (int i = 0; i < nout && i < 11; ++i) out[i] = v[i];
   });
 }
 
@@ -2210,12 +2425,17 @@ int fb_server_reset_clock(fb_server srv) {
     if (!srv) fail(FB_ERR_ARGUMENT, "null argument");
     cuda_check(cudaEventRecord(srv->start, srv->streams[0]), "event record");
     cuda_check(cudaEventSynchronize(srv->start), "event sync");
+    if (srv->clk_host) {
+      cuda_check(pq_clock(srv->streams[0], srv->clk_dev, srv->clk_host), "clock");
+      srv->clk0_ns = *(volatile int64_t*)srv->clk_host;
+    }
   });
 }
 
 int fb_server_destroy(fb_server srv) {
   return guard([&] {
     if (!srv) return;
+    srv->pq.reset();  // asks the resident kernel to stop and waits for it
     cudaDeviceSynchronize();
     delete srv;
   });

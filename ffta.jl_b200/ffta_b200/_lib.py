@@ -59,6 +59,7 @@ SIGNATURES = {
     "fb_server_poll": ([_vp, _i64, _i64p, ctypes.POINTER(ctypes.c_double), _i64p], ctypes.c_int),
     "fb_server_wait": ([_vp], ctypes.c_int),
     "fb_server_cancel": ([_vp, _i64], ctypes.c_int),
+    "fb_server_drop_next_descriptor": ([_vp], ctypes.c_int),
     "fb_server_stats": ([_vp, _i64p, ctypes.c_int], ctypes.c_int),
     "fb_server_reset_clock": ([_vp], ctypes.c_int),
     "fb_server_destroy": ([_vp], ctypes.c_int),

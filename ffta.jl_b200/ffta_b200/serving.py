@@ -38,7 +38,7 @@ import time
 
 import numpy as np
 
-from . import _lib, _check, plan_fft, plan_bfft, FB_SERVER_NO_GRAPHS
+from . import _lib, _check, plan_fft, plan_bfft, FB_SERVER_NO_GRAPHS, FB_SERVER_NO_PERSISTENT
 
 ELEM = {"c64": 8, "c128": 16}
 
@@ -258,13 +258,15 @@ class Server:
     CUDA graph captured on its second occurrence."""
 
     KIND = {"c64": _lib.FB_C32, "c128": _lib.FB_C64}
-    NSTATS = 8
+    NSTATS = 11
 
-    def __init__(self, budget_bytes: float = 100e9, nstreams: int = 4, graphs: bool = True):
+    def __init__(self, budget_bytes: float = 100e9, nstreams: int = 4, graphs: bool = True,
+                 resident: bool = True):
         self.budget = budget_bytes
         self.nstreams = nstreams
         self.h = ctypes.c_void_p()
-        flags = 0 if graphs else FB_SERVER_NO_GRAPHS
+        flags = (0 if graphs else FB_SERVER_NO_GRAPHS) | (0 if resident else
+                                                           FB_SERVER_NO_PERSISTENT)
         _check(_lib.lib.fb_server_create(ctypes.byref(self.h), float(budget_bytes), nstreams,
                                          flags))
 
@@ -346,7 +348,9 @@ class Server:
         out.update({"launches": st1[1] - st0[1], "descriptor_launches": st1[2] - st0[2],
                     "max_queue": st1[3], "max_admitted_GB": st1[4] / 1e9,
                     "resident_plans": st1[5], "graph_launches": st1[6] - st0[6],
-                    "graph_captures": st1[7] - st0[7], "streams": self.nstreams})
+                    "graph_captures": st1[7] - st0[7], "streams": self.nstreams,
+                    "resident_kernel_requests": st1[9] - st0[9],
+                    "failed_requests": st1[10] - st0[10]})
         return out
 
 

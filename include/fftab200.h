@@ -63,12 +63,16 @@ enum { FB_DEFAULT_BLUESTEIN_CUTOFF = 73 }; /* src/callgraph.jl:44 */
  *   (tcgen05, split-BF16 operands in three terms, FP32 accumulation) instead
  *   of the FP32 butterflies.  Error stays at the FP32 path's level; results
  *   are not bit-identical to the default path.  No FFTA counterpart (FFTA
- *   computes in the element type only). */
+ *   computes in the element type only).
+ * FB_FLAG_NO_TMA: load the tiles of strided passes (four-step columns,
+ *   strided axes) thread by thread instead of with tensor copies into shared
+ *   memory (bit-identical results; the flag exists so tests can check that). */
 enum {
   FB_FLAG_GENERIC_ONLY = 1u,
   FB_FLAG_SAME_SCHEDULE_STRIDED = 2u,
   FB_FLAG_STREAM = 4u,
-  FB_FLAG_TENSOR_STAGE = 8u
+  FB_FLAG_TENSOR_STAGE = 8u,
+  FB_FLAG_NO_TMA = 16u
 };
 
 /* Batched 1-D plan: `batch` transforms of length n; element j of transform b
@@ -152,8 +156,16 @@ int fb_execute_grouped(fb_plan plan, int64_t count, const void* const* ins, void
  * recurs is captured into a CUDA graph on its second occurrence and replayed
  * as one graph launch afterwards (at most 1024 graphs per server, least
  * recently used released first); FB_SERVER_NO_GRAPHS in `flags` turns this
- * off. */
-enum { FB_SERVER_NO_GRAPHS = 1u };
+ * off.
+ * Small requests of length 16..4096 (powers of two) go instead to one
+ * resident kernel: the server appends a work descriptor per request to a
+ * queue in mapped host memory, and the kernel -- launched when work arrives
+ * and none is resident, ending after 2 ms without new work -- claims chunks
+ * of lines of the queued requests with the specialised stage programs.  Its
+ * waits are bounded; a request whose descriptor does not arrive in time
+ * completes with done_ms = -1 in fb_server_poll.  FB_SERVER_NO_PERSISTENT
+ * sends those requests to the descriptor launches as well. */
+enum { FB_SERVER_NO_GRAPHS = 1u, FB_SERVER_NO_PERSISTENT = 2u };
 typedef struct fb_server_s* fb_server;
 int fb_server_create(fb_server* srv, double budget_bytes, int nstreams, uint32_t flags);
 /* Queue `batch` contiguous transforms of length n (device pointers; the
@@ -178,11 +190,18 @@ int fb_server_poll(fb_server srv, int64_t max, int64_t* tickets, double* done_ms
  * runs, its output is not written and poll never reports its ticket.
  * FB_ERR_ARGUMENT if the ticket is unknown, already dispatched or done. */
 int fb_server_cancel(fb_server srv, int64_t ticket);
+/* Diagnostic (failure-path tests): the next request the server sends to its
+ * resident kernel is published with a descriptor that never arrives, as if
+ * its write had been lost.  The kernel waits for it a bounded time (2 ms),
+ * gives up, completes it with done_ms = -1 and goes on with the others.
+ * FB_ERR_UNSUPPORTED without a resident kernel. */
+int fb_server_drop_next_descriptor(fb_server srv);
 /* Dispatch and wait until every submitted request has completed. */
 int fb_server_wait(fb_server srv);
-/* out[0..8]: requests, launches, descriptor launches, max queue depth, max
+/* out[0..10]: requests, launches, descriptor launches, max queue depth, max
  * admitted bytes, resident plans, graph launches, graph captures, cancelled
- * requests (the first `nout` of them). */
+ * requests, requests served by the resident kernel, requests it gave up on
+ * (the first `nout` of them). */
 int fb_server_stats(fb_server srv, int64_t* out, int nout);
 /* Restart the clock of fb_server_poll's completion times (waits until the
  * server's first stream is idle). */

@@ -120,3 +120,83 @@ def test_graph_cache_releases_least_recently_used():
     bwd = F.bfft(base.T, 1).T
     for i, y in enumerate(ys):
         assert torch.equal(y[0], (fwd if i % 2 else bwd)[i]), i
+
+
+@pytest.mark.gpu
+def test_resident_kernel_serves_small_requests():
+    """Small requests of lengths 16..4096 (powers of two) go to the resident
+    kernel: a persistent launch that claims chunks of queued work
+    descriptors.  Each result equals the plan's own specialised kernel bit
+    for bit and the FP64 oracle within tolerance; the kernel ends when idle
+    and is launched again for later requests."""
+    import time
+    import torch
+    import ffta_b200 as F
+    import oracle
+    rng = np.random.default_rng(21)
+    spec = [(int(2 ** rng.integers(4, 13)), "c64" if rng.random() < 0.7 else "c128",
+             -1 if rng.random() < 0.5 else 1, int(rng.integers(1, 40))) for _ in range(120)]
+    reqs = [serving.Request(i, n, k, d, b, i, 0.0) for i, (n, k, d, b) in enumerate(spec)]
+    xs = serving.make_inputs(reqs, "cuda")
+    srv = serving.Server(nstreams=2)
+    for rnd in range(2):
+        ys = [torch.full_like(x, float("nan")) for x in xs]
+        st = srv.run(reqs, xs, ys)
+        assert st["resident_kernel_requests"] == len(reqs) and st["failed_requests"] == 0, st
+        assert st["descriptor_launches"] == 0
+        for r, x, y in zip(reqs, xs, ys):
+            f = F.fft if r.dir < 0 else F.bfft
+            assert torch.equal(y, f(x.T, 1).T), r
+        for r, x, y in list(zip(reqs, xs, ys))[:12]:
+            ref = oracle.fft_nd(x.cpu().numpy().T, 1, r.dir, prec="f64").T
+            eps = 2.0 ** -23 if r.kind == "c64" else 2.0 ** -52
+            err = np.linalg.norm(y.cpu().numpy() - ref) / np.linalg.norm(ref)
+            assert err <= 4 * eps * max(1.0, np.log2(r.n)), (r, err)
+        time.sleep(0.05)  # the kernel ends after 2 ms without work
+
+
+@pytest.mark.gpu
+def test_resident_kernel_gives_up_on_a_lost_descriptor():
+    """A descriptor whose write is lost (fb_server_drop_next_descriptor): the
+    resident kernel waits for it a bounded time, completes it with
+    done_ms = -1 and serves the requests queued behind it."""
+    import ctypes
+    import torch
+    import oracle
+    from ffta_b200 import _lib
+    h = ctypes.c_void_p()
+    assert _lib.lib.fb_server_create(ctypes.byref(h), 8e9, 2, 0) == 0, _lib.last_error()
+    try:
+        g = torch.Generator(device="cuda").manual_seed(4)
+        xs = [torch.randn(8, 1024, dtype=torch.complex64, device="cuda", generator=g)
+              for _ in range(3)]
+        ys = [torch.full_like(x, float("nan")) for x in xs]
+        tk = ctypes.c_int64()
+        tickets = []
+        for i, (x, y) in enumerate(zip(xs, ys)):
+            if i == 1:
+                assert _lib.lib.fb_server_drop_next_descriptor(h) == 0
+            assert _lib.lib.fb_server_submit(h, 1024, _lib.FB_C32, -1, 8,
+                                             ctypes.c_void_p(x.data_ptr()),
+                                             ctypes.c_void_p(y.data_ptr()),
+                                             ctypes.byref(tk)) == 0, _lib.last_error()
+            tickets.append(tk.value)
+        assert _lib.lib.fb_server_wait(h) == 0, _lib.last_error()
+        tks = (ctypes.c_int64 * 8)()
+        tms = (ctypes.c_double * 8)()
+        cnt = ctypes.c_int64()
+        assert _lib.lib.fb_server_poll(h, 8, tks, tms, ctypes.byref(cnt)) == 0
+        done = dict(zip(tks[:cnt.value], tms[:cnt.value]))
+        assert sorted(done) == sorted(tickets)
+        assert done[tickets[1]] == -1.0 and done[tickets[0]] >= 0 and done[tickets[2]] >= 0
+        st = (ctypes.c_int64 * 11)()
+        assert _lib.lib.fb_server_stats(h, st, 11) == 0
+        assert st[9] == 3 and st[10] == 1
+        torch.cuda.synchronize()
+        assert torch.isnan(ys[1]).all()
+        for i in (0, 2):
+            ref = oracle.fft_batched(xs[i].cpu().numpy().astype(np.complex128), -1)
+            err = np.linalg.norm(ys[i].cpu().numpy() - ref) / np.linalg.norm(ref)
+            assert err <= 4 * 2.0 ** -23 * 10, err
+    finally:
+        _lib.lib.fb_server_destroy(h)
