@@ -591,6 +591,88 @@ __global__ void __launch_bounds__(TileThreads<R, T, MID>::value,
   }
 }
 
+// ------------------------------------------------------- real kernel
+// Half-length real transforms of contiguous lines of even length n = 2L, as
+// FFTA computes them (src/plan.jl:398-442 and :466-495, after Sorensen et
+// al.): rfft reads the real line as L complex values z[m] = x[2m] + i x[2m+1]
+// (no conversion pass), transforms them with the length-L program into
+// shared memory and splits Z into the n/2+1 outputs
+//   X[k]   = XX + w^k XY,  X[L-k] = conj(XX - w^k XY),
+//   XX = (Z[k] + conj Z[L-k]) / 2,  XY = i (conj Z[L-k] - Z[k]) / 2,
+//   X[0] = Re Z[0] + Im Z[0],  X[L] = Re Z[0] - Im Z[0],  w = exp(-2 pi i / n);
+// brfft builds Zb[k] = XX + i XY, Zb[L-k] = conj(XX - i XY) with
+// XX = Y[k] + conj Y[L-k], XY = w^-k (Y[k] - conj Y[L-k]) and
+// Zb[0] = (Re Y[0] + Re Y[L]) + i (Re Y[0] - Re Y[L]) in shared memory,
+// runs the inverse program and stores the L complex results as the 2L reals.
+// One HBM read and one write per element, as in the complex kernel, at half
+// its length.  w^k comes from a table computed in FP64 and rounded once.
+template <typename R, int DIR, class RL, int T>
+__global__ void __launch_bounds__(DirectBounds<R, T>::threads, DirectBounds<R, T>::min_blocks)
+    fast_real_kernel(const RealArgs a) {
+  typedef cplx<R> C;
+  typedef Sc<R> S;
+  constexpr int L = prog_len<RL>();
+  constexpr int LPAD = lpad_of(L);
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* buf = (C*)smraw + threadIdx.y * LPAD;
+  const int64_t line = (int64_t)blockIdx.x * a.G + threadIdx.y;
+  const bool ok = line < a.nlines;
+  const int64_t l = ok ? line : 0;
+  const int u = threadIdx.x;
+  const C* tw = (const C*)a.tw;
+  const R* pcs = (const R*)a.prime_cs;
+  const C* __restrict__ wk = (const C*)a.wk;
+  const R h = R(0.5), sc = (R)a.scale;
+  const bool cs = a.st_stream != 0;
+  if constexpr (DIR < 0) {
+    const DirectIn<R> in{(const C*)((const R*)a.in + l * a.idist), ok};
+    fast_prog<R, -1, RL, T>(buf, in, SmemIO{}, tw, pcs, u);
+    if (!ok) return;  // (no barrier follows)
+    C* o = (C*)a.out + l * a.odist;
+    for (int k = u; k <= L / 2; k += T) {
+      if (k == 0) {
+        const C z = buf[pidx<RL>(0)];
+        store<R>(o, S::mk(S::mul(S::add(z.x, z.y), sc), R(0)), cs);
+        store<R>(o + L, S::mk(S::mul(S::sub(z.x, z.y), sc), R(0)), cs);
+        continue;
+      }
+      const C A = buf[pidx<RL>(k)], B = buf[pidx<RL>(L - k)];
+      const C xx = S::mk(S::mul(h, S::add(A.x, B.x)), S::mul(h, S::sub(A.y, B.y)));
+      // XY = i * (conj B - A) / 2
+      const C xy = S::mk(S::mul(h, S::add(B.y, A.y)), S::mul(h, S::sub(B.x, A.x)));
+      const C wxy = cmul<R>(__ldg(wk + k), xy);
+      store<R>(o + k, cscale<R>(cadd<R>(xx, wxy), sc), cs);
+      if (k != L - k) {
+        const C d = csub<R>(xx, wxy);
+        store<R>(o + (L - k), cscale<R>(S::mk(d.x, -d.y), sc), cs);
+      }
+    }
+  } else {
+    const C* __restrict__ y = (const C*)a.in + l * a.idist;
+    for (int k = u; k <= L / 2; k += T) {
+      if (k == 0) {
+        const R a0 = ok ? __ldcs(y).x : R(0), aL = ok ? __ldcs(y + L).x : R(0);
+        buf[pidx<RL>(0)] = S::mk(S::add(a0, aL), S::sub(a0, aL));
+        continue;
+      }
+      const C A = ok ? __ldcs(y + k) : S::mk(R(0), R(0));
+      const C B = ok ? __ldcs(y + (L - k)) : S::mk(R(0), R(0));
+      const C xx = S::mk(S::add(A.x, B.x), S::sub(A.y, B.y));
+      const C dd = S::mk(S::sub(A.x, B.x), S::add(A.y, B.y));
+      const C xy = cmulc<R>(dd, __ldg(wk + k));  // w^-k (Y[k] - conj Y[L-k])
+      const C ixy = S::mk(-xy.y, xy.x);
+      buf[pidx<RL>(k)] = cadd<R>(xx, ixy);
+      if (k != L - k) {
+        const C d = csub<R>(xx, ixy);
+        buf[pidx<RL>(L - k)] = S::mk(d.x, -d.y);
+      }
+    }
+    __syncthreads();
+    const DirectOut<R> out{(C*)((R*)a.out + l * a.odist), ok, sc, cs};
+    fast_prog<R, 1, RL, T>(buf, SmemIO{}, out, tw, pcs, u);
+  }
+}
+
 // ------------------------------------------------------ TMA tile kernel
 // The lean tile kernel for passes whose lines are neighbours in memory
 // (four-step columns, strided 2-D axes): instead of each thread loading its
@@ -900,6 +982,34 @@ template <typename R, class RL, int T> struct FastEntry {
       k<<<dim3((unsigned)nblk), dim3(T), smem, s>>>(a);
       e = cudaGetLastError();
       if (e != cudaSuccess) launch_failure(k, "stream launch", L, T, 1, smem, e);
+      return e;
+    }
+  }
+  // Half-length real kernel: lines of 2L for L up to 8192 (one block of at
+  // most 512 threads per line).
+  static constexpr bool has_real = L >= 2 && T <= 512;
+  static cudaError_t launch_real(int dir, const RealArgs& a, cudaStream_t s) {
+    if constexpr (!has_real) {
+      snprintf(g_launch_msg, sizeof(g_launch_msg), "no real kernel for L=%d", L);
+      return cudaErrorNotSupported;
+    } else {
+      static int set_fwd[64] = {0}, set_bwd[64] = {0};
+      const size_t smem = (size_t)a.G * LPAD * sizeof(cplx<R>);
+      auto k = dir < 0 ? fast_real_kernel<R, -1, RL, T> : fast_real_kernel<R, 1, RL, T>;
+      if (a.G < 1 || a.G * T > DirectBounds<R, T>::threads) {
+        launch_failure(k, "real launch shape", L, T, a.G, smem, cudaErrorInvalidValue);
+        return cudaErrorInvalidValue;
+      }
+      cudaError_t e = configure(k, smem, dir < 0 ? set_fwd : set_bwd);
+      if (e != cudaSuccess) {
+        launch_failure(k, "real smem attribute", L, T, a.G, smem, e);
+        return e;
+      }
+      const int64_t nblk = (a.nlines + a.G - 1) / a.G;
+      if (nblk <= 0) return cudaSuccess;
+      k<<<dim3((unsigned)nblk), dim3(T, a.G), smem, s>>>(a);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) launch_failure(k, "real launch", L, T, a.G, smem, e);
       return e;
     }
   }

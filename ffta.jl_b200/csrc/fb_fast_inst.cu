@@ -29,6 +29,9 @@ namespace fb {
    FastEntry<FB_R, RList<__VA_ARGS__>, T>::TILE_THREADS,                      \
    FastEntry<FB_R, RList<__VA_ARGS__>, T>::has_tma                             \
        ? &FastEntry<FB_R, RList<__VA_ARGS__>, T>::launch_tile_tma              \
+       : nullptr,                                                              \
+   FastEntry<FB_R, RList<__VA_ARGS__>, T>::has_real                            \
+       ? &FastEntry<FB_R, RList<__VA_ARGS__>, T>::launch_real                  \
        : nullptr}
 
 static const FastFn kTable[] = {

@@ -125,6 +125,24 @@ constexpr uint64_t kWaitNsDefault = 1000000000ull;
 // The limit a launch uses: fb_set_wait_limit's value, 0 for the default.
 uint64_t wait_limit_ns();
 
+// Arguments of the half-length real kernel (fast_real_kernel): `nlines`
+// contiguous real lines of even length n = 2L.  rfft reads line l as L
+// complex values (even samples real, odd ones imaginary) at in + l*idist
+// reals, transforms them and splits the result into the n/2+1 outputs at
+// out + l*odist complex values; brfft does the reverse (idist complex in,
+// odist reals out).  FFTA src/plan.jl:398-442 (rfft) and :466-495 (brfft).
+struct RealArgs {
+  const void* in;
+  void* out;
+  int64_t nlines, idist, odist;
+  const void* tw;        // stage twiddles of the length-L program
+  const void* prime_cs;
+  const void* wk;        // exp(-2 pi i k / n), k = 0..L/2, FP64-made, rounded once
+  double scale;
+  int G;
+  int st_stream;
+};
+
 // Geometry of a tile pass whose loads are tensor copies (fast_tma_tile_kernel):
 // tile k holds lines k*G .. k*G+G-1 (G divides the first batch level, so a
 // tile's lines are neighbours in memory), brought into shared memory as
@@ -158,6 +176,9 @@ struct FastFn {
   // tiles in flight); `tmap` is the CUtensorMap of the pass's input;
   // nullptr where the length has none
   cudaError_t (*launch_tile_tma)(const LineArgs&, const void* tmap, const TmaGeom&, cudaStream_t);
+  // half-length real transform of lines of length 2L (dir -1: rfft, +1:
+  // brfft); nullptr where the length has none
+  cudaError_t (*launch_real)(int dir, const RealArgs&, cudaStream_t);
 };
 
 // Bytes of one direction's B table of the tensor-core radix-16 stage.
@@ -226,6 +247,17 @@ int pq_poll(PQueue* q, int64_t r, int64_t* t_ns, int32_t* status);
 // The device globaltimer, read by a one-thread kernel on `s` into mapped
 // host memory (device and host addresses of one int64).
 cudaError_t pq_clock(cudaStream_t s, int64_t* host_mapped_dev, int64_t* host_mapped);
+
+// Strided copy between two layouts of one array: element k (k_d < dims[d])
+// moves from in + sum k_d*is[d] to out + sum k_d*os[d] (strides in elements
+// of elem_bytes = 4, 8 or 16).
+struct PermCopy {
+  int rank;
+  int64_t dims[8], is[8], os[8];
+  int64_t count;
+};
+cudaError_t permute_copy(int elem_bytes, const void* in, void* out, const PermCopy& p,
+                         cudaStream_t s);
 
 // Real-transform helpers on contiguous column-major arrays (dtype 0: float /
 // ComplexF32, 1: double / ComplexF64).

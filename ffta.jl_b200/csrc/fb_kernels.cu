@@ -421,6 +421,35 @@ cudaError_t herm_extend(int dtype, const void* x, void* z, int rank, const int64
   return cudaGetLastError();
 }
 
+// out[sum_d k_d * os[d]] = in[sum_d k_d * is[d]] for every index (k_d < dims[d]):
+// a strided copy that moves an array between two layouts (rank <= 8).
+template <typename E>
+__global__ void k_permute(const E* __restrict__ in, E* __restrict__ out, PermCopy p) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < p.count;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t t = i, oi = 0, oo = 0;
+    for (int d = 0; d < p.rank; ++d) {
+      const int64_t k = t % p.dims[d];
+      t /= p.dims[d];
+      oi += k * p.is[d];
+      oo += k * p.os[d];
+    }
+    out[oo] = in[oi];
+  }
+}
+
+cudaError_t permute_copy(int elem_bytes, const void* in, void* out, const PermCopy& p,
+                         cudaStream_t s) {
+  if (p.count <= 0) return cudaSuccess;
+  switch (elem_bytes) {
+    case 4: k_permute<float><<<grid_for(p.count), 256, 0, s>>>((const float*)in, (float*)out, p); break;
+    case 8: k_permute<float2><<<grid_for(p.count), 256, 0, s>>>((const float2*)in, (float2*)out, p); break;
+    case 16: k_permute<double2><<<grid_for(p.count), 256, 0, s>>>((const double2*)in, (double2*)out, p); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t gen_prime_tables(void* f32tab, void* f64tab, cudaStream_t s) {
   const int total = prime_table_total();
   k_prime_tables<<<grid_for(total), 256, 0, s>>>((float*)f32tab, (double*)f64tab, total);

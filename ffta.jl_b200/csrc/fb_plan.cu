@@ -226,8 +226,45 @@ static int um_for(int R, int cap) { return R >= cap ? 1 : cap / R; }
 // Radix program for a length whose prime factors are all <= FB_MAX_PRIME:
 // powers of two as radix 16 with an 8, 4 or 2 (8*4 in place of 16*2), then
 // powers of three as radix 9 with a final 3, then fives and the odd primes
-// in ascending order.  The program depends on the length alone.
+// in ascending order.  The program depends on the length alone -- unless a
+// plan made with FB_FLAG_TUNE_RADIX has a tuned program for the length (the
+// override below, consulted while such a plan is built).
+static thread_local const std::map<int64_t, std::vector<int>>* g_radix_override = nullptr;
+// Tuned programs per (type, direction) and length: chosen by fb_plan_autotune
+// for plans with FB_FLAG_TUNE_RADIX, used by later such plans.
+static std::mutex g_radix_mu;
+static std::map<std::pair<int, int>, std::map<int64_t, std::vector<int>>> g_radix_tuned;
+// Sets the override for the plan being built and restores the caller's.
+struct RadixScope {
+  const std::map<int64_t, std::vector<int>>* saved;
+  std::map<int64_t, std::vector<int>> own;
+  RadixScope(int dtype, int dir, uint32_t flags, const std::map<int64_t, std::vector<int>>* force)
+      : saved(g_radix_override) {
+    if (force) {
+      own = *force;
+      g_radix_override = &own;
+    } else if (flags & FB_FLAG_TUNE_RADIX) {
+      std::lock_guard<std::mutex> lk(g_radix_mu);
+      own = g_radix_tuned[{dtype, dir}];
+      g_radix_override = &own;
+    } else {
+      g_radix_override = nullptr;
+    }
+  }
+  ~RadixScope() { g_radix_override = saved; }
+};
+// An explicit override for the next create_plan on this thread (the tuner's
+// candidates).
+static thread_local const std::map<int64_t, std::vector<int>>* g_radix_force = nullptr;
+static std::vector<int> default_radix_program(int64_t L);
 static std::vector<int> radix_program(int64_t L) {
+  if (g_radix_override) {
+    auto it = g_radix_override->find(L);
+    if (it != g_radix_override->end()) return it->second;
+  }
+  return default_radix_program(L);
+}
+static std::vector<int> default_radix_program(int64_t L) {
   std::vector<int> r;
   int a = 0;
   while (L % 2 == 0) {
@@ -388,10 +425,12 @@ struct Pass {
   int tc = 0;                      // 1: first radix-16 stage on the tensor cores
   int tma = 0;                     // 1: run `staged` fed by tensor copies (geometry tg)
   TmaGeom tg;
-  // the tensor map of the last input this pass ran on (re-encoded when the
-  // input address changes)
+  // the tensor map of the last input this pass ran on, with the box it was
+  // encoded for (re-encoded when the input address, the lines per tile or
+  // the box rows change -- the autotuner may change the lines per tile)
   CUtensorMap tmap;
   const void* tmap_in = nullptr;
+  int tmap_G = 0, tmap_boxr = 0;
 };
 
 // The specialised kernel for a radix program, if one is compiled.
@@ -444,6 +483,15 @@ struct fb_plan_s {
   int real_kind = 0;
   std::unique_ptr<fb_plan_s> cplan;
   std::unique_ptr<fb::DevBuf> zbuf;
+  // half-length real path (even length along the contiguous first dim):
+  // the real kernel's length-L program and arguments; cplan then covers the
+  // other region dims of the half array (or is null)
+  const fb::FastFn* rfn = nullptr;
+  fb::RealArgs ra;
+  // a strided region dim: the copies that bring it to the front and back
+  // (real array and half array) and the contiguous buffers between them
+  fb::PermCopy perm_full, perm_half;
+  std::unique_ptr<fb::DevBuf> zr, zc;
   int r0 = 0;
   int64_t rh = 0;
   uint32_t region_mask = 0;
@@ -548,9 +596,9 @@ static void use_tile(const fb_plan_s* P, Pass& p, const std::vector<int>& radice
 // whole 32-byte sectors and 16-byte units, and two tiles must fit in shared
 // memory.  Shared memory per block: up to ~110 KB (two blocks per SM) when
 // two or three buffers fit there, else up to ~220 KB (one block per SM).
-static bool tma_geometry(const fb_plan_s* P, const Pass& p, int G, TmaGeom* g) {
+static bool tma_geometry(const fb_plan_s* P, const Pass& p, const LineArgs& a, TmaGeom* g) {
   const FastFn* ff = p.staged;
-  const LineArgs& a = p.a;
+  const int G = a.G;
   if (!ff || !ff->launch_tile_tma || p.tc || !a.plain_io || a.mid) return false;
   if (a.ld.mode != 1 || a.ld.s0 != 1 || G < 2 || G * ff->T > ff->tile_threads) return false;
   const int es = elem_bytes(P->dtype);
@@ -573,7 +621,8 @@ static bool tma_geometry(const fb_plan_s* P, const Pass& p, int G, TmaGeom* g) {
   const size_t buf = (std::max(flat, padded) + 1023) / 1024 * 1024;
   int nbuf = (int)std::min<size_t>(3, (110 * 1024) / buf);
   if (nbuf < 2) nbuf = (int)std::min<size_t>(3, (220 * 1024) / buf);
-  if (nbuf < 2) return false;
+  if (getenv("FB_TMA_NBUF")) nbuf = std::min<int>(atoi(getenv("FB_TMA_NBUF")), (int)((220 * 1024) / buf));  // EXPERIMENT
+  if (nbuf < (getenv("FB_TMA_NBUF") ? 1 : 2)) return false;  // EXPERIMENT
   g->nbox = nbox;
   g->boxr = boxr;
   g->units = es / 8;
@@ -589,9 +638,28 @@ static bool tma_geometry(const fb_plan_s* P, const Pass& p, int G, TmaGeom* g) {
 static void plan_tma(const fb_plan_s* P, Pass& p) {
   if ((P->flags & FB_FLAG_NO_TMA) || !p.staged) return;
   const int es = elem_bytes(P->dtype);
+  const int pol = getenv("FB_TMA_POLICY") ? atoi(getenv("FB_TMA_POLICY")) : 1;  // EXPERIMENT
+  if (pol == 0) return;  // EXPERIMENT
+  int bestG = 0;
+  if (pol == 2) {  // EXPERIMENT: most resident warps per SM
+    double bw = 0;
+    for (int G = 128 / es; G * es >= 32; G /= 2) {
+      TmaGeom g;
+      LineArgs ag = p.a;
+      ag.G = G;
+      if (!tma_geometry(P, p, ag, &g)) continue;
+      const int thr = G * p.staged->T;
+      const int bs = std::min(std::min((int)((227 * 1024) / (g.nbuf * g.buf_bytes + 256)), 2048 / thr), 65536 / (thr * 64));
+      const double w = (double)bs * thr / 32 + G * 1e-3;
+      if (w > bw) { bw = w; bestG = G; }
+    }
+  }
   for (int G = 128 / es; G * es >= 32; G /= 2) {
     TmaGeom g;
-    if (!tma_geometry(P, p, G, &g)) continue;
+    if (bestG && G != bestG) continue;  // EXPERIMENT
+    LineArgs ag = p.a;
+    ag.G = G;
+    if (!tma_geometry(P, p, ag, &g)) continue;
     p.tma = 1;
     p.tg = g;
     p.a.G = G;
@@ -601,8 +669,9 @@ static void plan_tma(const fb_plan_s* P, Pass& p) {
 }
 
 // CUtensorMap of a tensor-copy pass over the input `in` (4-D: lines in
-// 8-byte units, elements, the two batch levels).
-static bool encode_tma(const fb_plan_s* P, Pass& p, const void* in) {
+// 8-byte units, elements, the two batch levels) with boxes of G lines x
+// g.boxr elements: the box the kernel's copies and byte counts assume.
+static bool encode_tma(const fb_plan_s* P, Pass& p, const void* in, int G, const TmaGeom& g) {
   typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                                const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
                                const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
@@ -619,7 +688,7 @@ static bool encode_tma(const fb_plan_s* P, Pass& p, const void* in) {
     cudaGetLastError();
   });
   if (!encode || reinterpret_cast<uintptr_t>(in) % 16) return false;
-  if (p.tmap_in == in) return true;
+  if (p.tmap_in == in && p.tmap_G == G && p.tmap_boxr == g.boxr) return true;
   const LineArgs& a = p.a;
   const int es = elem_bytes(P->dtype);
   const int64_t m2 = a.nlines / (a.m0 * a.m1);
@@ -630,14 +699,19 @@ static bool encode_tma(const fb_plan_s* P, Pass& p, const void* in) {
   const cuuint64_t s1 = a.m1 > 1 ? (cuuint64_t)(a.ld.s1 * es) : row * a.prog.L;
   const cuuint64_t s2 = m2 > 1 ? (cuuint64_t)(a.ld.s2 * es) : s1 * a.m1;
   const cuuint64_t strides[3] = {row, s1, s2};
-  const cuuint32_t box[4] = {(cuuint32_t)(a.G * (es / 8)), (cuuint32_t)p.tg.boxr, 1, 1};
+  const cuuint32_t box[4] = {(cuuint32_t)(G * (es / 8)), (cuuint32_t)g.boxr, 1, 1};
   const cuuint32_t estr[4] = {1, 1, 1, 1};
   const CUresult r =
       encode(&p.tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<void*>(in), dims, strides,
              box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return false;
+  if (r != CUDA_SUCCESS) {
+    p.tmap_in = nullptr;
+    return false;
+  }
   p.tmap_in = in;
+  p.tmap_G = G;
+  p.tmap_boxr = g.boxr;
   return true;
 }
 
@@ -684,7 +758,8 @@ static fb_plan_s* create_plan(int dtype, int dir, int rank, const int64_t* dims,
                               const int64_t* istrides, const int64_t* ostrides,
                               const std::vector<int>& region, int64_t cutoff,
                               uint32_t flags = 0);
-static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s);
+static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s,
+                         int64_t nb = -1);
 
 // Chirp spectrum FFT_M(b_ext), forward, computed in FP64 by a C64 plan and
 // rounded to the plan type, optionally scaled.
@@ -1267,6 +1342,7 @@ static Axis plan_axis(fb_plan_s* P, int64_t n, int64_t is, int64_t os, std::vect
       // as the first pass (the strided columns)
       c *= 1.0 + 1e-9 * std::fabs(std::log((double)a) - std::log((double)b));
       if ((a & (a - 1)) == 0 && (b & (b - 1)) != 0) c *= 1.0 - 1e-6;
+      if (getenv("FB_FOUR_N1") && a == atoll(getenv("FB_FOUR_N1"))) c = 0;  // EXPERIMENT
       if (c < best) {
         best = c;
         bN1 = a;
@@ -1288,6 +1364,11 @@ static fb_plan_s* create_plan(int dtype, int dir, int rank, const int64_t* dims,
     fail(FB_ERR_ARGUMENT, "element type must be ComplexF32 or ComplexF64");
   if (dir != FB_FORWARD && dir != FB_BACKWARD) fail(FB_ERR_ARGUMENT, "direction must be -1 or +1");
   if (rank < 1) fail(FB_ERR_DIMENSION_MISMATCH, "array must have at least one dimension");
+  // radix programs: tuned ones for FB_FLAG_TUNE_RADIX plans, the tuner's
+  // candidate while it times one, else the defaults
+  const auto* force = g_radix_force;
+  g_radix_force = nullptr;
+  RadixScope radix_scope(dtype, dir, flags, force);
   for (size_t i = 0; i < region.size(); ++i) {
     if (region[i] < 0 || region[i] >= rank)
       fail(FB_ERR_DIMENSION_MISMATCH, "Plan region is outside array dimensions.");
@@ -1365,7 +1446,20 @@ static fb_plan_s* create_plan(int dtype, int dir, int rank, const int64_t* dims,
 
 static void execute_real(fb_plan_s* P, const void* in, void* out, cudaStream_t s);
 
-static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s) {
+// Whether a plan is a batched 1-D plan over contiguous-or-strided lines with
+// one batch dim (fb_plan_create), which fb_execute_batch can run on fewer
+// transforms than it was made for.
+static bool batched_1d(const fb_plan_s* P) {
+  return !P->real_kind && P->rank == 2 && P->region.size() == 1 && P->region[0] == 0 &&
+         P->axes.size() == 1 && P->axes[0].outer.size() <= 1;
+}
+
+// nb >= 0 (batched 1-D plans only): run the first nb transforms of the
+// batch.  The axis covers Bin transforms per host-loop step (the whole batch,
+// or one L2 chunk); every pass's lines are a whole multiple of Bin, so a
+// step of bc < Bin transforms runs nlines / Bin * bc lines.
+static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s,
+                         int64_t nb) {
   if (P->real_kind) {
     execute_real(P, in, out, s);
     return;
@@ -1378,6 +1472,11 @@ static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s
     Axis& ax = P->axes[ai];
     int64_t nouter = 1;
     for (auto& o : ax.outer) nouter *= o.n;
+    int64_t Bin = 0;
+    if (nb >= 0) {
+      Bin = P->dims[1] / nouter;
+      nouter = (nb + Bin - 1) / Bin;
+    }
     for (int64_t oi = 0; oi < nouter; ++oi) {
       int64_t offi = 0, offo = 0, t = oi;
       for (auto& o : ax.outer) {
@@ -1386,9 +1485,14 @@ static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s
         offi += k * o.is;
         offo += k * o.os;
       }
+      const int64_t bc = nb >= 0 ? std::min(Bin, nb - oi * Bin) : 0;
       for (size_t pi = 0; pi < ax.passes.size(); ++pi) {
         Pass& p = ax.passes[pi];
         LineArgs a = p.a;
+        if (nb >= 0) {
+          a.nlines = p.a.nlines / Bin * bc;
+          if (a.nlines <= 0) continue;
+        }
         auto resolve = [&](int id, int64_t off) -> void* {
           switch (id) {
             case B_IN: return (char*)in + off * es;
@@ -1411,6 +1515,7 @@ static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s
           fa.out = a.out;
           fa.st_stream = a.st_stream;
           fa.wait_ns = a.wait_ns;
+          if (nb >= 0) fa.nlines = p.fa.nlines / Bin * bc;
           if (last) fa.scale = P->scale;
           // the bulk copies need 16-byte aligned line starts
           const bool st = p.stream && p.fast->launch_stream &&
@@ -1426,7 +1531,7 @@ static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s
           // tensor copies need the geometry for the current lines per tile
           // (the autotuner may have changed them) and a 16-byte aligned input
           TmaGeom tg;
-          if (p.tma && tma_geometry(P, p, a.G, &tg) && encode_tma(P, p, a.in)) {
+          if (p.tma && tma_geometry(P, p, a, &tg) && encode_tma(P, p, a.in, a.G, tg)) {
             const cudaError_t e = p.staged->launch_tile_tma(a, &p.tmap, tg, s);
             if (e != cudaSuccess) cuda_check(e, last_launch_message());
             continue;
@@ -1515,6 +1620,21 @@ int fb_execute(fb_plan plan, const void* in, void* out, void* stream) {
     if (!plan) fail(FB_ERR_ARGUMENT, "null plan");
     if ((!in || !out) && (plan->in_span > 0)) fail(FB_ERR_ARGUMENT, "null data pointer");
     execute_plan(plan, in, out, (cudaStream_t)stream);
+  });
+}
+
+int fb_execute_batch(fb_plan plan, const void* in, void* out, int64_t batch, void* stream) {
+  return guard([&] {
+    if (!plan) fail(FB_ERR_ARGUMENT, "null plan");
+    if (!batched_1d(plan))
+      fail(FB_ERR_UNSUPPORTED, "fb_execute_batch takes a batched 1-D plan (fb_plan_create)");
+    if (batch < 0 || batch > plan->dims[1])
+      fail(FB_ERR_DIMENSION_MISMATCH, "batch " + std::to_string(batch) +
+                                          " is outside the plan's 0.." +
+                                          std::to_string(plan->dims[1]));
+    if (batch == 0) return;
+    if (!in || !out) fail(FB_ERR_ARGUMENT, "null data pointer");
+    execute_plan(plan, in, out, (cudaStream_t)stream, batch);
   });
 }
 
@@ -1677,6 +1797,18 @@ int fb_plan_describe(fb_plan plan, char* buf, size_t len) {
     if (!plan || !buf || !len) fail(FB_ERR_ARGUMENT, "null argument");
     std::ostringstream o;
     o << (plan->dtype == FB_C32 ? "C32" : "C64") << (plan->dir < 0 ? " fwd" : " bwd");
+    if (plan->real_kind) {
+      o << (plan->real_kind == 1 ? " rfft" : " brfft");
+      if (plan->rfn)
+        o << " | n=" << plan->dims[plan->r0] << " REAL-HALF(L=" << plan->rfn->L
+          << " T=" << plan->rfn->T << " G=" << plan->ra.G << (plan->zr ? " strided" : "") << ")";
+      else
+        o << " | full-length complex plan:";
+      if (plan->cplan) {
+        char sub[3000];
+        if (fb_plan_describe(plan->cplan.get(), sub, sizeof(sub)) == FB_OK) o << " + " << sub;
+      }
+    }
     for (auto& ax : plan->axes) {
       o << " | n=" << ax.n << " " << ax.kind;
       if (!ax.outer.empty()) o << " (host loop " << ax.outer.size() << " dims)";
@@ -1732,6 +1864,125 @@ const char* fb_version(void) { return FB_VERSION; }
 // rounding.
 namespace fb {
 
+// FFTA's even-length real transform (src/plan.jl:398-442, :466-495): when
+// the first region dim is the contiguous one (dim 1) and has even length
+// n = 2L whose half runs on a specialised kernel, one fast_real_kernel pass
+// transforms every line at half length with the split fused in, and the
+// other region dims (if any) are complex transforms of the n/2+1-long half
+// array -- after the real pass for rfft (in place on the output), before it
+// for brfft (input -> scratch).  Returns nullptr when the path does not apply.
+static fb_plan_s* create_half_real_plan(int dtype, int dir, int rank, const int64_t* dims,
+                                        const std::vector<int>& region, int64_t cutoff,
+                                        uint32_t flags) {
+  if (region.empty() || (flags & FB_FLAG_GENERIC_ONLY)) return nullptr;
+  // a single strided region dim is moved to the front (a strided copy in
+  // and out), so every 1-D real transform takes the same half-length path
+  // as a contiguous vector -- FFTA applies its vector method to each slice
+  // (mapslices, src/plan.jl:507-527) -- and gives the same bits
+  const int r0 = region[0];
+  if (r0 != 0 && region.size() != 1) return nullptr;
+  const int64_t n = dims[r0];
+  if (n < 4 || n % 2) return nullptr;
+  int64_t total = 1;
+  for (int d = 0; d < rank; ++d) total *= dims[d];
+  if (total <= 0) return nullptr;
+  const int64_t L = n / 2;
+  LineX x;
+  if (!make_direct(L, cutoff, dtype, &x) || x.kind != 0) return nullptr;
+  const FastFn* ff = find_fast(dtype, (int)L, x.radices);
+  if (!ff || !ff->launch_real || (int)ff->lpad != lpad_for((int)L)) return nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    fail(FB_ERR_CUDA, "no CUDA device: this library has no CPU fallback");
+  }
+  std::unique_ptr<fb_plan_s> P(new fb_plan_s());
+  P->dtype = dtype;
+  P->dir = dir;
+  P->cutoff = cutoff;
+  P->flags = flags;
+  P->rank = rank;
+  P->dims.assign(dims, dims + rank);
+  std::vector<int64_t> st(rank), hd(dims, dims + rank), hst(rank);
+  hd[r0] = L + 1;
+  int64_t s = 1, hs = 1;
+  for (int d = 0; d < rank; ++d) {
+    st[d] = s;
+    hst[d] = hs;
+    s *= dims[d];
+    hs *= hd[d];
+  }
+  P->istrides = st;
+  P->ostrides = st;
+  P->region = region;
+  cuda_check(cudaGetDevice(&P->device), "cudaGetDevice");
+  P->real_kind = dir == FB_FORWARD ? 1 : 2;
+  P->r0 = r0;
+  P->rh = L + 1;
+  for (int r : region) P->region_mask |= 1u << r;
+  const int64_t half = total / n * (L + 1);
+  if (r0 != 0) {
+    // dims in the order (r0, the others): the kernel's contiguous lines
+    std::vector<int> perm{r0};
+    for (int d = 0; d < rank; ++d)
+      if (d != r0) perm.push_back(d);
+    PermCopy full, hp;
+    memset(&full, 0, sizeof(full));
+    memset(&hp, 0, sizeof(hp));
+    full.rank = hp.rank = rank;
+    full.count = total;
+    hp.count = half;
+    int64_t cf = 1, ch = 1;
+    for (int d = 0; d < rank; ++d) {
+      full.dims[d] = dims[perm[d]];
+      hp.dims[d] = hd[perm[d]];
+      // real array: `st` (user layout) <-> contiguous (cf); half: hst <-> ch
+      full.is[d] = P->real_kind == 1 ? st[perm[d]] : cf;
+      full.os[d] = P->real_kind == 1 ? cf : st[perm[d]];
+      hp.is[d] = P->real_kind == 1 ? ch : hst[perm[d]];
+      hp.os[d] = P->real_kind == 1 ? hst[perm[d]] : ch;
+      cf *= full.dims[d];
+      ch *= hp.dims[d];
+    }
+    P->perm_full = full;
+    P->perm_half = hp;
+    P->zr.reset(new DevBuf((size_t)total * elem_bytes(dtype) / 2));
+    P->zc.reset(new DevBuf((size_t)half * elem_bytes(dtype)));
+  }
+  P->in_span = P->real_kind == 1 ? total : half;
+  P->out_span = P->real_kind == 1 ? half : total;
+  // the length-L program and the split's twiddles w^k = exp(-2 pi i k / n)
+  StageProg prog;
+  fill_prog(P.get(), x, &prog);
+  void* wk = alloc_table(P.get(), (size_t)(L / 2 + 1) * elem_bytes(dtype));
+  cuda_check(gen_roots(dtype, wk, n, 1, L / 2 + 1, 0), "real split twiddles");
+  RealArgs& a = P->ra;
+  memset(&a, 0, sizeof(a));
+  a.nlines = total / n;
+  a.idist = P->real_kind == 1 ? n : L + 1;
+  a.odist = P->real_kind == 1 ? L + 1 : n;
+  a.tw = prog.tw;
+  const DeviceTables& dt = device_tables(P->device);
+  a.prime_cs = dtype == FB_C32 ? dt.f32 : dt.f64;
+  a.wk = wk;
+  a.scale = 1.0;
+  // lines per block as for the complex direct kernel: up to a warp's worth
+  // of threads, within 100 KB of shared memory
+  int G = std::max(1, 32 / ff->T);
+  while (G > 1 && (size_t)G * ff->lpad * elem_bytes(dtype) > 100 * 1024) G /= 2;
+  while (G > 1 && G / 2 >= a.nlines) G /= 2;
+  a.G = G;
+  P->rfn = ff;
+  if (region.size() > 1) {
+    std::vector<int> reg(region.begin() + 1, region.end());
+    P->cplan.reset(create_plan(dtype, dir, rank, hd.data(), hst.data(), hst.data(), reg, cutoff,
+                               flags));
+    if (P->real_kind == 2) P->zbuf.reset(new DevBuf((size_t)half * elem_bytes(dtype)));
+  }
+  cuda_check(cudaStreamSynchronize(0), "real plan tables");
+  return P.release();
+}
+
 static fb_plan_s* create_real_plan(int dtype, int dir, int rank, const int64_t* dims,
                                    const std::vector<int>& region, int64_t cutoff, uint32_t flags) {
   if (region.empty()) fail(FB_ERR_ARGUMENT, "a real transform needs at least one region dim");
@@ -1742,6 +1993,7 @@ static fb_plan_s* create_real_plan(int dtype, int dir, int rank, const int64_t* 
     st[d] = total;
     total *= dims[d];
   }
+  if (auto* H = create_half_real_plan(dtype, dir, rank, dims, region, cutoff, flags)) return H;
   std::unique_ptr<fb_plan_s> C(create_plan(dtype, dir, rank, dims, st.data(), st.data(), region,
                                            cutoff, flags));
   std::unique_ptr<fb_plan_s> P(new fb_plan_s());
@@ -1776,6 +2028,59 @@ static void execute_real(fb_plan_s* P, const void* in, void* out, cudaStream_t s
     if (d > P->r0) post *= P->dims[d];
   }
   if (total == 0) return;
+  if (P->rfn && P->zr) {
+    // strided region dim: copy to (r0, others) order, transform, copy back
+    RealArgs a = P->ra;
+    const int es = elem_bytes(P->dtype);
+    a.scale = P->scale;
+    a.st_stream = 0;
+    if (P->real_kind == 1) {
+      cuda_check(permute_copy(es / 2, in, P->zr->p, P->perm_full, s), "real gather");
+      a.in = P->zr->p;
+      a.out = P->zc->p;
+    } else {
+      cuda_check(permute_copy(es, in, P->zc->p, P->perm_half, s), "half gather");
+      a.in = P->zc->p;
+      a.out = P->zr->p;
+    }
+    const cudaError_t e = P->rfn->launch_real(P->real_kind == 1 ? FB_FORWARD : FB_BACKWARD, a, s);
+    if (e != cudaSuccess) cuda_check(e, last_launch_message());
+    if (P->real_kind == 1)
+      cuda_check(permute_copy(es, P->zc->p, out, P->perm_half, s), "half scatter");
+    else
+      cuda_check(permute_copy(es / 2, P->zr->p, out, P->perm_full, s), "real scatter");
+    return;
+  }
+  if (P->rfn) {
+    RealArgs a = P->ra;
+    fb_plan_s* C = P->cplan.get();
+    if (P->real_kind == 1) {
+      a.in = in;
+      a.out = out;
+      a.scale = C ? 1.0 : P->scale;
+      a.st_stream = C ? 0 : 1;
+      const cudaError_t e = P->rfn->launch_real(FB_FORWARD, a, s);
+      if (e != cudaSuccess) cuda_check(e, last_launch_message());
+      if (C) {
+        C->scale = P->scale;
+        execute_plan(C, out, out, s);
+      }
+    } else {
+      const void* src = in;
+      if (C) {
+        C->scale = 1.0;
+        execute_plan(C, in, P->zbuf->p, s);
+        src = P->zbuf->p;
+      }
+      a.in = src;
+      a.out = out;
+      a.scale = P->scale;
+      a.st_stream = 1;
+      const cudaError_t e = P->rfn->launch_real(FB_BACKWARD, a, s);
+      if (e != cudaSuccess) cuda_check(e, last_launch_message());
+    }
+    return;
+  }
   P->cplan->scale = P->scale;
   void* z = P->zbuf->p;
   if (P->real_kind == 1) {
@@ -1836,6 +2141,7 @@ struct SrvReq {
   void* out;
   double bytes;
   const SrvShape* shape;  // nullptr: multi-pass length
+  bool drop = false;      // fault injection: its descriptor never arrives
 };
 
 struct SrvLaunch {
@@ -1905,7 +2211,7 @@ struct fb_server_s {
   int64_t* clk_host = nullptr;  // mapped pinned: globaltimer at the clock origin
   int64_t* clk_dev = nullptr;
   int64_t clk0_ns = 0;
-  int64_t pq_seq_add = 0;  // fault injection (tests): next descriptor never arrives
+  bool drop_next = false;  // fault injection (tests): the next request's descriptor never arrives
   double st_max_admitted = 0;
   ~fb_server_s() {
     for (auto& g : graph_of) cudaGraphExecDestroy(g.second.exec);
@@ -2150,8 +2456,9 @@ static void srv_dispatch(fb_server_s* S) {
         cuda_check(pq_set_program(S->pq.get(), pid, tp.a.prog.tw, tp.a.prime_cs),
                    "resident program table");
       }
-      const int64_t q = pq_push(S->pq.get(), pid, r.in, r.out, r.batch, S->pq_seq_add);
-      S->pq_seq_add = 0;
+      // a dropped descriptor carries a sequence number no request ever has
+      const int64_t q =
+          pq_push(S->pq.get(), pid, r.in, r.out, r.batch, r.drop ? int64_t(1) << 41 : 0);
       S->pq_out.push_back({q, r.ticket, r.bytes});
       S->st_resident += 1;
       resident = true;
@@ -2288,7 +2595,7 @@ int fb_server_create(fb_server* srv, double budget_bytes, int nstreams, uint32_t
     cuda_check(cudaEventSynchronize(S->start), "event sync");
     if (!(flags & FB_SERVER_NO_PERSISTENT)) {
       PQueue* q = nullptr;
-      cuda_check(pq_create(&q, 2000000), "persistent queue");  // ends after 2 ms idle
+      cuda_check(pq_create(&q, getenv("FB_PQ_IDLE_US") ? 1000ull * atoi(getenv("FB_PQ_IDLE_US")) : 100000ull), "persistent queue");  // EXPERIMENT
       S->pq.reset(q);
       cuda_check(cudaHostAlloc((void**)&S->clk_host, sizeof(int64_t), cudaHostAllocMapped),
                  "clock");
@@ -2326,7 +2633,8 @@ int fb_server_submit(fb_server srv, int64_t n, int dtype, int dir, int64_t batch
     if (!shape) bytes += (double)plan_scratch_bytes(srv_multi(srv, n, dtype, dir, batch));
     // a request that could never be admitted is refused now, not queued for good
     if (bytes > srv->budget) refuse();
-    SrvReq r{srv->next_ticket++, n, batch, dtype, dir, in, out, bytes, shape};
+    SrvReq r{srv->next_ticket++, n, batch, dtype, dir, in, out, bytes, shape, srv->drop_next};
+    srv->drop_next = false;
     srv->pending.push_back(r);
     srv->st_requests += 1;
     srv->st_max_queue = std::max<int64_t>(srv->st_max_queue, (int64_t)srv->pending.size());
@@ -2367,7 +2675,7 @@ int fb_server_drop_next_descriptor(fb_server srv) {
   return guard([&] {
     if (!srv) fail(FB_ERR_ARGUMENT, "null argument");
     if (!srv->pq) fail(FB_ERR_UNSUPPORTED, "the server has no resident kernel");
-    srv->pq_seq_add = int64_t(1) << 41;  // a sequence number no request ever has
+    srv->drop_next = true;
   });
 }
 
@@ -2577,6 +2885,70 @@ static void apply_tuning(fb_plan_s* P) {
   for (size_t i = 0; i < ps.size(); ++i) set_shape(*ps[i], pick[i]);
 }
 
+// Alternative radix programs of a one-pass length L: groupings of the factor
+// 2^a into radices 16/8/4/2 (largest first; fewest stages first), of 3^b into
+// 9/3, the other primes ascending; the powers of two first, or (when both
+// are present) the powers of three first.  The default program comes first;
+// at most 12, each one a program the kernels can run.
+static std::vector<std::vector<int>> radix_candidates(int64_t L, int dtype) {
+  int a = 0, b = 0;
+  int64_t m = L;
+  while (m % 2 == 0) {
+    m /= 2;
+    ++a;
+  }
+  while (m % 3 == 0) {
+    m /= 3;
+    ++b;
+  }
+  std::vector<int> rest;
+  for (auto& pe : factorize(m))
+    for (int i = 0; i < pe.second; ++i) rest.push_back((int)pe.first);
+  std::vector<std::vector<int>> p2;
+  std::vector<int> cur;
+  std::function<void(int, int)> part = [&](int left, int maxlg) {
+    if (left == 0) {
+      p2.push_back(cur);
+      return;
+    }
+    for (int lg = std::min(maxlg, left); lg >= 1; --lg) {
+      cur.push_back(1 << lg);
+      part(left - lg, lg);
+      cur.pop_back();
+    }
+  };
+  part(a, 4);
+  std::stable_sort(p2.begin(), p2.end(),
+                   [](const std::vector<int>& x, const std::vector<int>& y) { return x.size() < y.size(); });
+  if (p2.size() > 5) p2.resize(5);
+  std::vector<std::vector<int>> p3;
+  for (int i = b / 2; i >= 0 && p3.size() < 2; --i) {
+    std::vector<int> v(i, 9);
+    v.insert(v.end(), b - 2 * i, 3);
+    p3.push_back(v);
+  }
+  std::vector<std::vector<int>> out{default_radix_program(L)};
+  auto add = [&](std::vector<int> v) {
+    v.insert(v.end(), rest.begin(), rest.end());
+    int T, var;
+    if ((int)v.size() > FB_MAX_STAGES || !pick_threads((int)L, v, &T, &var)) return;
+    if (std::find(out.begin(), out.end(), v) == out.end() && out.size() < 12) out.push_back(v);
+  };
+  for (auto& x : p2)
+    for (auto& y : p3) {
+      std::vector<int> v = x;
+      v.insert(v.end(), y.begin(), y.end());
+      add(v);
+      if (!x.empty() && !y.empty()) {
+        std::vector<int> w = y;
+        w.insert(w.end(), x.begin(), x.end());
+        add(w);
+      }
+    }
+  (void)dtype;
+  return out;
+}
+
 static double time_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t st, int iters) {
   cudaEvent_t e0, e1;
   cuda_check(cudaEventCreate(&e0), "event");
@@ -2593,6 +2965,59 @@ static double time_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t st
   return ms / std::max(1, iters);
 }
 
+// FB_FLAG_TUNE_RADIX: for every one-pass length of the plan, build the plan
+// with each candidate program for that length, time it on the caller's
+// buffers and keep the fastest (its schedule replaces the plan's own); the
+// choice is recorded for later plans with the flag.
+static void tune_radix(fb_plan_s* P, const void* in, void* out, cudaStream_t st, int iters) {
+  std::vector<int64_t> Ls;
+  for (auto& ax : P->axes)
+    if (ax.kind == "DIRECT" && ax.passes.size() == 1 && ax.n > 3 &&
+        std::find(Ls.begin(), Ls.end(), ax.n) == Ls.end())
+      Ls.push_back(ax.n);
+  std::map<int64_t, std::vector<int>> chosen;
+  {
+    std::lock_guard<std::mutex> lk(g_radix_mu);
+    chosen = g_radix_tuned[{P->dtype, P->dir}];
+  }
+  for (int64_t L : Ls) {
+    const auto cands = radix_candidates(L, P->dtype);
+    if (cands.size() < 2) continue;
+    double tbest = time_plan(P, in, out, st, iters);
+    std::unique_ptr<fb_plan_s> best;
+    std::vector<int> bestc;
+    for (const auto& c : cands) {
+      std::map<int64_t, std::vector<int>> ov = chosen;
+      ov[L] = c;
+      g_radix_force = &ov;
+      std::unique_ptr<fb_plan_s> Q(create_plan(P->dtype, P->dir, P->rank, P->dims.data(),
+                                               P->istrides.data(), P->ostrides.data(), P->region,
+                                               P->cutoff, P->flags));
+      Q->scale = P->scale;
+      const double t = time_plan(Q.get(), in, out, st, iters);
+      if (t < tbest) {
+        tbest = t;
+        best = std::move(Q);
+        bestc = c;
+      }
+    }
+    if (best) {
+      chosen[L] = bestc;
+      std::swap(P->axes, best->axes);
+      std::swap(P->bufs, best->bufs);
+      std::swap(P->table_bytes, best->table_bytes);
+      std::swap(P->scratch_elems, best->scratch_elems);
+      std::swap(P->scratch0, best->scratch0);
+      std::swap(P->scratch1, best->scratch1);
+      P->chunk_plan.reset();  // the host pipeline's plans are made again
+      P->tail_plan.reset();
+    }
+  }
+  std::lock_guard<std::mutex> lk(g_radix_mu);
+  auto& g = g_radix_tuned[{P->dtype, P->dir}];
+  for (auto& kv : chosen) g[kv.first] = kv.second;
+}
+
 }  // namespace fb
 
 extern "C" {
@@ -2605,6 +3030,7 @@ int fb_plan_autotune(fb_plan plan, const void* in, void* out, void* stream, int 
     if (!in || !out) fail(FB_ERR_ARGUMENT, "null data pointer");
     cudaStream_t st = (cudaStream_t)stream;
     iters = std::max(1, iters);
+    if (plan->flags & FB_FLAG_TUNE_RADIX) tune_radix(plan, in, out, st, iters);
     auto ps = all_passes(plan);
     for (Pass* p : ps) {
       auto shapes = pass_shapes(plan, *p);
@@ -2638,13 +3064,21 @@ int fb_tune_cache_save(const char* path) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     FILE* f = std::fopen(path, "w");
     if (!f) fail(FB_ERR_ARGUMENT, std::string("cannot write ") + path);
-    std::fprintf(f, "# fftab200 tuning cache v1: key|G,T,variant;...\n");
+    std::fprintf(f, "# fftab200 tuning cache v1: key|G,T,variant;...  and  radix|type:dir:L|r.r.r\n");
     for (auto& kv : g_tune) {
       std::fprintf(f, "%s|", kv.first.c_str());
       for (size_t i = 0; i < kv.second.G.size(); ++i)
         std::fprintf(f, "%d,%d,%d;", kv.second.G[i], kv.second.T[i], kv.second.variant[i]);
       std::fprintf(f, "\n");
     }
+    std::lock_guard<std::mutex> lr(g_radix_mu);
+    for (auto& td : g_radix_tuned)
+      for (auto& kv : td.second) {
+        std::fprintf(f, "radix|%d:%d:%lld|", td.first.first, td.first.second, (long long)kv.first);
+        for (size_t i = 0; i < kv.second.size(); ++i)
+          std::fprintf(f, "%s%d", i ? "." : "", kv.second[i]);
+        std::fprintf(f, "\n");
+      }
     std::fclose(f);
   });
 }
@@ -2659,6 +3093,27 @@ int fb_tune_cache_load(const char* path) {
     while (std::fgets(line, sizeof(line), f)) {
       std::string l(line);
       if (l.empty() || l[0] == '#') continue;
+      if (l.compare(0, 6, "radix|") == 0) {
+        // a tuned radix program: kept only if it multiplies to its length
+        int dt, dr;
+        long long L;
+        if (std::sscanf(l.c_str() + 6, "%d:%d:%lld|", &dt, &dr, &L) != 3) continue;
+        std::istringstream rs(l.substr(l.find('|', 6) + 1));
+        std::vector<int> prog;
+        std::string tok;
+        int64_t prod = 1;
+        while (std::getline(rs, tok, '.')) {
+          const int r = std::atoi(tok.c_str());
+          if (r < 2 || r > FB_MAX_PRIME) break;
+          prog.push_back(r);
+          prod *= r;
+        }
+        if (prod == L && !prog.empty() && prog.size() <= FB_MAX_STAGES) {
+          std::lock_guard<std::mutex> lr(g_radix_mu);
+          g_radix_tuned[{dt, dr}][L] = prog;
+        }
+        continue;
+      }
       const size_t bar = l.find('|');
       if (bar == std::string::npos) continue;
       TuneEntry e;

@@ -458,7 +458,7 @@ cudaError_t pq_create(PQueue** out, uint64_t idle_ns) {
   a.progs = (const PProg*)(d + off_prog);
   a.idle_ns = idle_ns;
   a.desc_wait_ns = 2000000;  // 2 ms
-  q->nblocks = std::min(per_sm, 2) * nsm;
+  q->nblocks = std::min(per_sm, getenv("FB_PQ_BPS") ? atoi(getenv("FB_PQ_BPS")) : 1) * nsm;  // EXPERIMENT
   *out = q;
   return cudaSuccess;
 }

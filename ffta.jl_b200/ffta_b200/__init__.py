@@ -329,6 +329,7 @@ FB_FLAG_SAME_SCHEDULE_STRIDED = 2  # strided axes bit-identical to contiguous on
 FB_FLAG_STREAM = 4  # persistent bulk-copy kernel for contiguous lines (bit-identical)
 FB_FLAG_TENSOR_STAGE = 8  # C32: first radix-16 stage on the tensor cores (split BF16)
 FB_FLAG_NO_TMA = 16  # strided passes load thread by thread, not by tensor copies
+FB_FLAG_TUNE_RADIX = 32  # autotune also chooses the radix program (results not bitwise equal)
 FB_SERVER_NO_GRAPHS = 1  # fb_server_create: no CUDA-graph replay of recurring multi-pass requests
 FB_SERVER_NO_PERSISTENT = 2  # fb_server_create: no resident kernel; small requests in descriptor launches
 
@@ -552,6 +553,12 @@ class FFTAPlan_re:
     def _regions(self):
         r = self.region
         return [r] if isinstance(r, int) else list(r)
+
+    def describe(self, dims) -> str:
+        """The device schedule for a real array of `dims` (Julia order)."""
+        buf = ctypes.create_string_buffer(8192)
+        _check(lib.fb_plan_describe(self._handle(tuple(int(d) for d in dims)), buf, len(buf)))
+        return buf.value.decode()
 
     def _handle(self, dims):
         h = self._cplans.get(dims)

@@ -41,6 +41,7 @@ SIGNATURES = {
     "fb_plan_set_scale": ([_vp, ctypes.c_double], ctypes.c_int),
     "fb_execute": ([_vp, _vp, _vp, _vp], ctypes.c_int),
     "fb_execute_host": ([_vp, _vp, _vp, _vp], ctypes.c_int),
+    "fb_execute_batch": ([_vp, _vp, _vp, _i64, _vp], ctypes.c_int),
     "fb_execute_grouped": ([_vp, _i64, ctypes.POINTER(_vp), ctypes.POINTER(_vp), _i64p, _vp],
                            ctypes.c_int),
     "fb_plan_size": ([_vp, ctypes.c_int, _i64p], ctypes.c_int),

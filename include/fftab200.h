@@ -66,13 +66,22 @@ enum { FB_DEFAULT_BLUESTEIN_CUTOFF = 73 }; /* src/callgraph.jl:44 */
  *   computes in the element type only).
  * FB_FLAG_NO_TMA: load the tiles of strided passes (four-step columns,
  *   strided axes) thread by thread instead of with tensor copies into shared
- *   memory (bit-identical results; the flag exists so tests can check that). */
+ *   memory (bit-identical results; the flag exists so tests can check that).
+ * FB_FLAG_TUNE_RADIX: let fb_plan_autotune also choose the radix program
+ *   (the order and sizes of the butterfly stages) of each one-pass length of
+ *   the plan among alternatives -- 16/8/4/2 groupings of the factor 2^a,
+ *   9/3 of 3^b, powers of two or of three first -- and use the tuned
+ *   programs in later plans made with this flag.  A tuned plan's results
+ *   are within the usual rounding of the default plan's, not bit-identical to
+ *   them.  No FFTA counterpart (FFTA's recursion order is fixed by its call
+ *   graph, src/callgraph.jl:76-126). */
 enum {
   FB_FLAG_GENERIC_ONLY = 1u,
   FB_FLAG_SAME_SCHEDULE_STRIDED = 2u,
   FB_FLAG_STREAM = 4u,
   FB_FLAG_TENSOR_STAGE = 8u,
-  FB_FLAG_NO_TMA = 16u
+  FB_FLAG_NO_TMA = 16u,
+  FB_FLAG_TUNE_RADIX = 32u
 };
 
 /* Batched 1-D plan: `batch` transforms of length n; element j of transform b
@@ -127,6 +136,14 @@ int fb_plan_set_scale(fb_plan plan, double scale);
  * is the legacy default stream).  Input and output may be the same buffer.
  * Replaces LinearAlgebra.mul!(y, p, x) (src/plan.jl:157,170,210,260). */
 int fb_execute(fb_plan plan, const void* in, void* out, void* stream);
+
+/* Run a batched 1-D plan (fb_plan_create) on its first `batch` transforms
+ * only (0 <= batch <= the plan's batch, else FB_ERR_DIMENSION_MISMATCH), with
+ * the plan's strides and distances: LinearAlgebra.mul! on the leading
+ * columns of the array, FFTA src/plan.jl:170-207.  Results equal those of
+ * the full plan for those columns bit for bit.  Lets a caller keep one plan
+ * per length for every batch up to its own (the serving loop does). */
+int fb_execute_batch(fb_plan plan, const void* in, void* out, int64_t batch, void* stream);
 
 /* Run the plan on host arrays: copies in, transforms, copies out, and returns
  * when `out` holds the result.  Pinned host memory gives full copy speed.
@@ -244,7 +261,9 @@ int fb_execute_noalloc_c32(const void* in, void* out, int64_t n, int64_t batch, 
  * per line -- on the given device buffers (their contents are overwritten),
  * keeps the fastest, and caches it for later plans of this process with the
  * same type, direction, dims, strides and region.  The stage program of a
- * length (its radix order) is not tuned, so results do not change. */
+ * length (its radix order) is not tuned, so results do not change -- unless
+ * the plan was made with FB_FLAG_TUNE_RADIX, which also times alternative
+ * radix programs of each one-pass length and keeps the fastest. */
 int fb_plan_autotune(fb_plan plan, const void* in, void* out, void* stream, int iters);
 /* Save / load the process-wide tuning cache (a text file).  Loaded entries
  * are applied only where every shape is valid for the plan's kernels. */

@@ -80,3 +80,45 @@ def test_autotune_generic_only_plan():
     before = (p * x).cpu()
     F.autotune(p, x, iters=2)
     assert torch.equal((p * x).cpu(), before)
+
+
+def _radices(desc):
+    import re
+    return re.findall(r"radices=([0-9x]+)", desc)
+
+
+@pytest.mark.gpu
+def test_radix_order_tuning():
+    """FB_FLAG_TUNE_RADIX: the tuner also times alternative radix programs of
+    each one-pass length (16/8/4/2 groupings of 2^a, 9/3 of 3^b, powers of
+    two or of three first) and keeps the fastest, per (length, type,
+    direction); later plans with the flag start from it.  A tuned plan is
+    not bit-identical to the default one, so results are checked against the
+    FP64 oracle within 4 eps log2 N.  Lengths without a specialised kernel
+    (generic runtime programs) are where the order matters most."""
+    import os
+    import torch
+    import oracle
+    shapes = [((224, 512), "c64"), ((448, 256), "c64"), ((1792, 64), "c64"), ((352, 512), "c64"),
+              ((2592, 64), "c64"), ((864, 128), "c128"), ((3584, 64), "c64"), ((4096, 256), "c64")]
+    changed = []
+    for shape, kind in shapes:
+        dt = torch.complex64 if kind == "c64" else torch.complex128
+        x = _column_major(shape, dt, shape[0])
+        p = F.plan_fft(x, 1, _flags=F.FB_FLAG_TUNE_RADIX)
+        d0 = p.describe(x)
+        F.autotune(p, x, iters=5)
+        d1 = p.describe(x)
+        ref = oracle.fft_nd(x.cpu().numpy().astype(np.complex128), 1, -1, prec="f64",
+                            nthreads=os.cpu_count() or 1)
+        y = (p * x).cpu().numpy()
+        eps = 2.0 ** -23 if kind == "c64" else 2.0 ** -52
+        err = np.linalg.norm(y - ref) / np.linalg.norm(ref)
+        assert err <= 4 * eps * np.log2(shape[0]), (shape, d1, err)
+        if _radices(d0) != _radices(d1):
+            changed.append((shape, _radices(d0), _radices(d1)))
+            # a new plan with the flag starts from the tuned program
+            q = F.plan_fft(x, 1, _flags=F.FB_FLAG_TUNE_RADIX)
+            assert _radices(q.describe(x)) == _radices(d1)
+            assert _radices(F.plan_fft(x, 1).describe(x)) == _radices(d0)  # default untouched
+    assert changed, "the default program won for every length"

@@ -484,3 +484,39 @@ def test_config4_2d(m, n):
     y = F.fft(t.T).T.cpu().numpy()
     ref = oracle.fft(np.asfortranarray(X.T.astype(np.complex128)), nthreads=NTHR).T
     assert relerr(y, ref) <= tol(np.complex64, m * n)
+
+
+@pytest.mark.parametrize("n,B,dtype", [(4096, 8, np.complex64), (2 ** 20, 16, np.complex64),
+                                       (27648, 7, np.complex128), (1000003, 3, np.complex64),
+                                       (1009, 9, np.complex64), (24576, 5, np.complex64)])
+def test_execute_batch_prefix(n, B, dtype):
+    """fb_execute_batch runs a batched plan on its first `batch` columns
+    (mul! on the leading columns): the same bits as the full plan there,
+    nothing written beyond -- across direct, four-step (L2-chunked), and
+    Bluestein schedules."""
+    import ctypes
+    import torch
+    from ffta_b200 import _lib
+    rng = np.random.default_rng(n + B)
+    x = torch.from_numpy(crandn(rng, (B, n), dtype)).cuda()
+    h = ctypes.c_void_p()
+    dt = _lib.FB_C32 if dtype == np.complex64 else _lib.FB_C64
+    assert _lib.lib.fb_plan_create(ctypes.byref(h), n, dt, -1, B, 1, n, 1, n, 73, 0) == 0
+    try:
+        full = torch.empty_like(x)
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        assert _lib.lib.fb_execute(h, ctypes.c_void_p(x.data_ptr()),
+                                   ctypes.c_void_p(full.data_ptr()), st) == 0
+        for nb in sorted({1, B // 2 + 1, B}):
+            y = torch.full_like(x, float("nan"))
+            assert _lib.lib.fb_execute_batch(h, ctypes.c_void_p(x.data_ptr()),
+                                             ctypes.c_void_p(y.data_ptr()), nb, st) == 0, \
+                _lib.last_error()
+            torch.cuda.synchronize()
+            assert torch.equal(y[:nb], full[:nb]), nb
+            assert torch.isnan(y[nb:]).all(), nb
+        bad = _lib.lib.fb_execute_batch(h, ctypes.c_void_p(x.data_ptr()),
+                                        ctypes.c_void_p(full.data_ptr()), B + 1, st)
+        assert bad == _lib.FB_ERR_DIMENSION_MISMATCH
+    finally:
+        _lib.lib.fb_plan_destroy(h)

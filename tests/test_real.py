@@ -186,3 +186,60 @@ def test_real_on_device_tensors():
     assert relerr(y, ref) <= tol("f32", 1000)
     back = F.irfft(F.rfft(t.T, 1), 1000, 1).T.cpu().numpy()
     assert relerr(back, x) <= 10 * tol("f32", 1000)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [4, 6, 18, 64, 1000, 2048, 4096, 8192, 16384])
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_half_length_path(n, prec):
+    """Even lengths whose half has a specialised kernel take FFTA's
+    half-length algorithm (src/plan.jl:398-442 rfft, :466-495 brfft): the
+    real line read as n/2 complex values, one kernel at half length with the
+    split fused in.  Checked against the oracle's complex transform of the
+    real input, by round trip, and bitwise against the same transform of
+    each column alone."""
+    import torch
+    import oracle
+    dt = torch.float32 if prec == "f32" else torch.float64
+    B = 7
+    g = torch.Generator(device="cuda").manual_seed(n)
+    x = torch.randn(B, n, dtype=dt, device="cuda", generator=g)  # columns of a Julia n x B
+    p = F.plan_rfft(x.T, 1)
+    assert "REAL-HALF" in p.describe((n, B)), p.describe((n, B))
+    y = p * x.T
+    ref = oracle.fft_batched(x.cpu().numpy().astype(np.complex128), -1,
+                             nthreads=NTHR)[:, : n // 2 + 1]
+    assert relerr(y.T.cpu().numpy(), ref) <= tol(prec, n)
+    for b in (0, B - 1):
+        assert torch.equal(y[:, b], F.rfft(x[b].clone()))
+    pb = F.plan_brfft(y, n, 1)
+    assert "REAL-HALF" in pb.describe((n, B))
+    z = F.irfft(y, n, 1)
+    assert relerr(z.T.cpu().numpy(), x.cpu().numpy()) <= 10 * tol(prec, n)
+    zb = pb * y
+    refb = n * x.cpu().numpy()
+    assert relerr(zb.T.cpu().numpy(), refb) <= 10 * tol(prec, n)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,r", [((6, 64, 5), 2), ((3, 4, 2048), 3), ((16, 30), 2)])
+def test_half_length_strided_region(shape, r):
+    """A single strided region dim takes the same half-length kernel (its
+    lines copied to the front and back), so it equals the transform of each
+    slice alone bit for bit, as FFTA's mapslices does (src/plan.jl:507-527)."""
+    import oracle
+    rng = np.random.default_rng(sum(shape))
+    x = np.asfortranarray(rng.standard_normal(shape).astype(np.float32))
+    n = shape[r - 1]
+    p = F.plan_rfft(x, r)
+    assert "REAL-HALF" in p.describe(shape) and "strided" in p.describe(shape)
+    y = F.rfft(x, r)
+    refs = np.apply_along_axis(lambda v: F.rfft(np.ascontiguousarray(v)), r - 1, x)
+    assert np.array_equal(y, refs)
+    ref = oracle.fft(x.astype(np.complex128), r, nthreads=NTHR)
+    ref = np.take(ref, range(n // 2 + 1), axis=r - 1)
+    assert relerr(y, ref) <= tol("f32", n)
+    b = F.brfft(y, n, r)
+    refb = np.apply_along_axis(lambda v: F.brfft(np.ascontiguousarray(v), n), r - 1, y)
+    assert np.array_equal(b, refb)
+    assert relerr(F.irfft(y, n, r), x) <= 10 * tol("f32", n)
