@@ -1184,6 +1184,28 @@ static Axis plan_blue3_axis(fb_plan_s* P, int64_t N, int64_t is, int64_t os,
   ax.kind = "BLUE3";
   std::vector<BDim> inner;
   split_levels(bd, 2, &inner, &ax.outer);
+  if (!inner.empty()) {
+    // as in the four-step: the batch in chunks whose scratch (M * chunk
+    // elements per buffer) is at most kL2Chunk, one after the other, so the
+    // scratch stays bounded (and in L2 between the passes)
+    const int64_t B0c = inner[0].n;
+    const int64_t per =
+        std::max<int64_t>(1, (int64_t)(kL2Chunk / ((size_t)M * elem_bytes(P->dtype))));
+    if (B0c > per) {
+      int64_t chunk = 1;
+      for (int64_t c = per; c >= 1; --c)
+        if (B0c % c == 0) {
+          chunk = c;
+          break;
+        }
+      if (chunk * 4 >= per) {
+        ax.outer.insert(ax.outer.begin(),
+                        BDim{B0c / chunk, chunk * inner[0].is, chunk * inner[0].os});
+        inner[0].n = chunk;
+        ax.kind = "BLUE3/L2";
+      }
+    }
+  }
   const int64_t B = prod_n(inner, 0, 2), B0 = level_n(inner, 0);
   P->scratch_elems = std::max<size_t>(P->scratch_elems, (size_t)(M * B));
   void* pre = alloc_table(P, (size_t)N * elem_bytes(P->dtype));
@@ -2168,10 +2190,25 @@ struct fb_server_s {
   // then never used by two launches at once); different plans run side by side
   std::vector<cudaStream_t> multi_streams;
   std::map<const fb_plan_s*, int> multi_stream_of;
+  int next_multi_stream = 0;
   cudaEvent_t start = nullptr;
   int next_stream = 0, next_slot = 0;
   std::map<std::tuple<int64_t, int, int>, std::unique_ptr<fb_plan_s>> templ;
-  std::map<std::tuple<int64_t, int, int, int64_t>, std::unique_ptr<fb_plan_s>> multi;
+  // plans of multi-pass and large requests, one per (n, type, direction,
+  // batch bucket) -- the bucket is the smallest power of two >= the batch,
+  // at least kSrvMinBucket -- run on a request's batch with the plan's
+  // variable-batch execution; least recently used plans are released while
+  // their device bytes exceed multi_cap
+  struct MultiPlan {
+    std::unique_ptr<fb_plan_s> P;
+    int64_t used = 0;
+    cudaEvent_t ev = nullptr;  // after its last launch
+    size_t bytes = 0;
+  };
+  std::map<std::tuple<int64_t, int, int, int64_t>, MultiPlan> multi;
+  size_t multi_bytes = 0, multi_cap = 0;
+  int64_t multi_clock = 0, st_plans_made = 0, st_plans_released = 0;
+  bool serial = false;  // FB_SERVER_SERIAL: one request at a time
   std::deque<fb::SrvReq> pending;
   std::deque<fb::SrvLaunch> inflight;
   std::vector<fb::SrvSlot> slots;
@@ -2183,7 +2220,7 @@ struct fb_server_s {
   // CUDA graphs of multi-pass plans keyed by (plan, input, output): a request
   // shape that recurs on the same buffers is captured on its second
   // occurrence and replayed as one graph launch from then on
-  typedef std::tuple<const fb_plan_s*, const void*, void*> GraphKey;
+  typedef std::tuple<const fb_plan_s*, const void*, void*, int64_t> GraphKey;
   struct Graph {
     cudaGraphExec_t exec;
     cudaStream_t st;
@@ -2225,6 +2262,8 @@ struct fb_server_s {
       if (sl.host) cudaFreeHost(sl.host);
     }
     pq.reset();
+    for (auto& m : multi)
+      if (m.second.ev) cudaEventDestroy(m.second.ev);
     if (clk_host) cudaFreeHost(clk_host);
     for (auto s : streams) cudaStreamDestroy(s);
     for (auto s : multi_streams) cudaStreamDestroy(s);
@@ -2253,14 +2292,48 @@ static bool srv_single_pass(const fb_plan_s* P) {
          P->axes[0].passes[0].a.ld.mode == 0 && P->axes[0].passes[0].a.st.mode == 0;
 }
 
+static const int64_t kSrvMinBucket = 512;
+static int64_t srv_bucket(int64_t batch) {
+  int64_t b = kSrvMinBucket;
+  while (b < batch) b *= 2;
+  return b;
+}
+static size_t plan_scratch_bytes(const fb_plan_s* P);
+static void srv_release_plan(fb_server_s* S, const fb_plan_s* P);
+
 static fb_plan_s* srv_multi(fb_server_s* S, int64_t n, int dtype, int dir, int64_t batch) {
-  auto key = std::make_tuple(n, dtype, dir, batch);
+  auto key = std::make_tuple(n, dtype, dir, srv_bucket(batch));
   auto it = S->multi.find(key);
-  if (it != S->multi.end()) return it->second.get();
-  int64_t dims[2] = {n, batch}, st[2] = {1, n};
+  if (it != S->multi.end()) {
+    it->second.used = ++S->multi_clock;
+    return it->second.P.get();
+  }
+  // over the cap: release idle plans, least recently used first
+  while (S->multi_bytes > S->multi_cap && !S->multi.empty()) {
+    auto lru = S->multi.end();
+    for (auto m = S->multi.begin(); m != S->multi.end(); ++m) {
+      if (m->second.ev && cudaEventQuery(m->second.ev) == cudaErrorNotReady) {
+        cudaGetLastError();
+        continue;
+      }
+      if (lru == S->multi.end() || m->second.used < lru->second.used) lru = m;
+    }
+    if (lru == S->multi.end()) break;  // every plan is busy
+    srv_release_plan(S, lru->second.P.get());
+    S->multi_bytes -= lru->second.bytes;
+    if (lru->second.ev) cudaEventDestroy(lru->second.ev);
+    S->multi.erase(lru);
+    S->st_plans_released += 1;
+  }
+  int64_t dims[2] = {n, srv_bucket(batch)}, st[2] = {1, n};
   std::vector<int> reg{0};
   fb_plan_s* P = create_plan(dtype, dir, 2, dims, st, st, reg, FB_DEFAULT_BLUESTEIN_CUTOFF, 0);
-  S->multi[key].reset(P);
+  fb_server_s::MultiPlan& m = S->multi[key];
+  m.P.reset(P);
+  m.used = ++S->multi_clock;
+  m.bytes = P->table_bytes + plan_scratch_bytes(P);
+  S->multi_bytes += m.bytes;
+  S->st_plans_made += 1;
   return P;
 }
 
@@ -2269,6 +2342,23 @@ static size_t plan_scratch_bytes(const fb_plan_s* P) {
   if (P->scratch0) b += P->scratch0->bytes;
   if (P->scratch1) b += P->scratch1->bytes;
   return b;
+}
+
+// Forget everything that refers to an idle plan about to be released: its
+// CUDA graphs (their launches have completed), its occurrence counts and its
+// plan stream.
+static void srv_release_plan(fb_server_s* S, const fb_plan_s* P) {
+  for (auto g = S->graph_of.begin(); g != S->graph_of.end();) {
+    if (std::get<0>(g->first) == P) {
+      cudaGraphExecDestroy(g->second.exec);
+      g = S->graph_of.erase(g);
+    } else {
+      ++g;
+    }
+  }
+  for (auto k = S->seen.begin(); k != S->seen.end();)
+    k = std::get<0>(k->first) == P ? S->seen.erase(k) : std::next(k);
+  S->multi_stream_of.erase(P);
 }
 
 // Graphs kept per server; the least recently used one is released first.
@@ -2296,17 +2386,17 @@ static void srv_sweep_graphs(fb_server_s* S) {
 // Capture only records the launches (relaxed mode, nothing runs), so the
 // graph's kernels and arguments are exactly those of execute_plan.
 static void srv_run_plan(fb_server_s* S, fb_plan_s* P, const void* in, void* out,
-                         cudaStream_t st) {
+                         int64_t batch, cudaStream_t st) {
   if (!S->graphs) {
-    execute_plan(P, in, out, st);
+    execute_plan(P, in, out, st, batch);
     return;
   }
-  const fb_server_s::GraphKey key(P, in, out);
+  const fb_server_s::GraphKey key(P, in, out, batch);
   auto g = S->graph_of.find(key);
   if (g == S->graph_of.end()) {
     if (S->seen.size() >= 16 * kGraphCacheMax) S->seen.clear();
     if (++S->seen[key] < 2) {
-      execute_plan(P, in, out, st);
+      execute_plan(P, in, out, st, batch);
       return;
     }
     if (S->graph_of.size() >= kGraphCacheMax) {
@@ -2324,7 +2414,7 @@ static void srv_run_plan(fb_server_s* S, fb_plan_s* P, const void* in, void* out
     cudaGraph_t graph = nullptr;
     cuda_check(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed), "graph capture");
     try {
-      execute_plan(P, in, out, st);
+      execute_plan(P, in, out, st, batch);
     } catch (...) {
       cudaStreamEndCapture(st, &graph);
       if (graph) cudaGraphDestroy(graph);
@@ -2428,7 +2518,9 @@ static const int64_t kPackedMaxElems = int64_t(1) << 18;
 
 static void srv_dispatch(fb_server_s* S) {
   std::vector<SrvReq> batch;
-  while (!S->pending.empty() && batch.size() < kDispatchMax) {
+  // serial mode: one request, and only once the previous one has completed
+  const size_t most = S->serial ? (S->inflight.empty() && S->pq_out.empty() ? 1 : 0) : kDispatchMax;
+  while (!S->pending.empty() && batch.size() < most) {
     const SrvReq& r = S->pending.front();
     if (S->admitted + r.bytes > S->budget && (S->admitted > 0 || !batch.empty())) break;
     S->admitted += r.bytes;
@@ -2464,15 +2556,21 @@ static void srv_dispatch(fb_server_s* S) {
       resident = true;
       continue;
     }
-    if (!r.shape) {
+    if (!r.shape || S->serial) {
       fb_plan_s* P = srv_multi(S, r.n, r.dtype, r.dir, r.batch);
       auto ms = S->multi_stream_of.find(P);
       if (ms == S->multi_stream_of.end())
         ms = S->multi_stream_of
-                 .emplace(P, (int)(S->multi_stream_of.size() % S->multi_streams.size()))
+                 .emplace(P, (int)(S->next_multi_stream++ % S->multi_streams.size()))
                  .first;
       cudaStream_t mst = S->multi_streams[ms->second];
-      srv_run_plan(S, P, r.in, r.out, mst);
+      srv_run_plan(S, P, r.in, r.out, r.batch, mst);
+      {
+        fb_server_s::MultiPlan& m =
+            S->multi[std::make_tuple(r.n, r.dtype, r.dir, srv_bucket(r.batch))];
+        if (!m.ev) cuda_check(cudaEventCreateWithFlags(&m.ev, cudaEventDisableTiming), "event");
+        cuda_check(cudaEventRecord(m.ev, mst), "event record");
+      }
       SrvLaunch l;
       cuda_check(cudaEventCreateWithFlags(&l.ev, cudaEventDefault), "event");
       cuda_check(cudaEventRecord(l.ev, mst), "event record");
@@ -2568,7 +2666,9 @@ int fb_server_create(fb_server* srv, double budget_bytes, int nstreams, uint32_t
     std::unique_ptr<fb_server_s> S(new fb_server_s());
     cuda_check(cudaGetDevice(&S->device), "cudaGetDevice");
     S->budget = budget_bytes > 0 ? budget_bytes : 100e9;
-    S->graphs = !(flags & FB_SERVER_NO_GRAPHS);
+    S->serial = (flags & FB_SERVER_SERIAL) != 0;
+    S->graphs = !(flags & FB_SERVER_NO_GRAPHS) && !S->serial;
+    S->multi_cap = (size_t)std::max(S->budget / 4, 1e9);
     const int ns = std::max(1, std::min(nstreams, 16));
     for (int i = 0; i < ns; ++i) {
       cudaStream_t st;
@@ -2593,7 +2693,7 @@ int fb_server_create(fb_server* srv, double budget_bytes, int nstreams, uint32_t
     cuda_check(cudaEventCreate(&S->start), "event");
     cuda_check(cudaEventRecord(S->start, S->streams[0]), "event record");
     cuda_check(cudaEventSynchronize(S->start), "event sync");
-    if (!(flags & FB_SERVER_NO_PERSISTENT)) {
+    if (!(flags & (FB_SERVER_NO_PERSISTENT | FB_SERVER_SERIAL))) {
       PQueue* q = nullptr;
       cuda_check(pq_create(&q, getenv("FB_PQ_IDLE_US") ? 1000ull * atoi(getenv("FB_PQ_IDLE_US")) : 100000ull), "persistent queue");  // EXPERIMENT
       S->pq.reset(q);
@@ -2719,12 +2819,13 @@ int fb_server_wait(fb_server srv) {
 int fb_server_stats(fb_server srv, int64_t* out, int nout) {
   return guard([&] {
     if (!srv || !out) fail(FB_ERR_ARGUMENT, "null argument");
-    const int64_t v[11] = {srv->st_requests, srv->st_launches, srv->st_desc_launches,
+    const int64_t v[13] = {srv->st_requests, srv->st_launches, srv->st_desc_launches,
                            srv->st_max_queue, (int64_t)srv->st_max_admitted,
                            (int64_t)(srv->templ.size() + srv->multi.size()),
                            srv->st_graph_launches, srv->st_graph_captures, srv->st_cancelled,
-                           srv->st_resident, srv->st_failed};
-    for (int i = 0; i < nout && i < 11; ++i) out[i] = v[i];
+                           srv->st_resident, srv->st_failed, srv->st_plans_made,
+                           srv->st_plans_released};
+    for (int i = 0; i < nout && i < 13; ++i) out[i] = v[i];
   });
 }
 

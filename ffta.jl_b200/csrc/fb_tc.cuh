@@ -49,6 +49,19 @@ __device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity) {
       : "memory");
   return done != 0;
 }
+// Non-blocking: has phase `parity` of *b completed?  (try_wait above may
+// suspend the thread for a while before it answers.)
+__device__ __forceinline__ bool mbar_peek(uint64_t* b, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_addr(b)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
 __device__ __forceinline__ uint64_t global_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -57,7 +70,7 @@ __device__ __forceinline__ uint64_t global_ns() {
 // Wait for phase `parity` of *b for at most `limit_ns` (0: kWaitNsDefault);
 // false if it gave up.  The iteration count is bounded as well.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, uint64_t limit_ns = 0) {
-  if (mbar_test(b, parity)) return true;
+  if (mbar_peek(b, parity)) return true;
   const uint64_t lim = limit_ns ? limit_ns : kWaitNsDefault;
   const uint64_t t0 = global_ns();
   for (uint32_t it = 0; it < (1u << 30); ++it) {

@@ -332,6 +332,7 @@ FB_FLAG_NO_TMA = 16  # strided passes load thread by thread, not by tensor copie
 FB_FLAG_TUNE_RADIX = 32  # autotune also chooses the radix program (results not bitwise equal)
 FB_SERVER_NO_GRAPHS = 1  # fb_server_create: no CUDA-graph replay of recurring multi-pass requests
 FB_SERVER_NO_PERSISTENT = 2  # fb_server_create: no resident kernel; small requests in descriptor launches
+FB_SERVER_SERIAL = 4  # fb_server_create: one request at a time, one plan launch each (the plain path)
 
 
 def plan_fft(x, region=None, *, BLUESTEIN_CUTOFF=DEFAULT_BLUESTEIN_CUTOFF, _flags=0, **_kwargs):

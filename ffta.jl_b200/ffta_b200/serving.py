@@ -38,7 +38,8 @@ import time
 
 import numpy as np
 
-from . import _lib, _check, plan_fft, plan_bfft, FB_SERVER_NO_GRAPHS, FB_SERVER_NO_PERSISTENT
+from . import (_lib, _check, plan_fft, plan_bfft, FB_SERVER_NO_GRAPHS, FB_SERVER_NO_PERSISTENT,
+               FB_SERVER_SERIAL)
 
 ELEM = {"c64": 8, "c128": 16}
 
@@ -258,15 +259,16 @@ class Server:
     CUDA graph captured on its second occurrence."""
 
     KIND = {"c64": _lib.FB_C32, "c128": _lib.FB_C64}
-    NSTATS = 11
+    NSTATS = 13
 
     def __init__(self, budget_bytes: float = 100e9, nstreams: int = 4, graphs: bool = True,
-                 resident: bool = True):
+                 resident: bool = True, serial: bool = False):
         self.budget = budget_bytes
         self.nstreams = nstreams
         self.h = ctypes.c_void_p()
-        flags = (0 if graphs else FB_SERVER_NO_GRAPHS) | (0 if resident else
-                                                           FB_SERVER_NO_PERSISTENT)
+        self.serial = serial
+        flags = ((0 if graphs else FB_SERVER_NO_GRAPHS) |
+                 (0 if resident else FB_SERVER_NO_PERSISTENT) | (FB_SERVER_SERIAL if serial else 0))
         _check(_lib.lib.fb_server_create(ctypes.byref(self.h), float(budget_bytes), nstreams,
                                          flags))
 
@@ -404,7 +406,7 @@ def compare_graphs(count=600, seed=13, nstreams=4, repeats=5):
 
 
 def compare(count=400, rates=(2000.0,), seed=11, n_max=2 ** 20, batch_max=512,
-            max_elems=1 << 22, budget_bytes=100e9, nstreams=4):
+            max_elems=1 << 22, budget_bytes=100e9, nstreams=4, resident=True):
     """Serve one trace with both paths at each arrival rate of a sweep.
 
     Requests whose n * batch exceeds `max_elems` get their batch reduced so the
@@ -423,7 +425,7 @@ def compare(count=400, rates=(2000.0,), seed=11, n_max=2 ** 20, batch_max=512,
     warm_plans(base, cache)
     xs = make_inputs(base, "cuda")
     ys = [torch.empty_like(x) for x in xs]
-    srv = Server(budget_bytes, nstreams)
+    srv = Server(budget_bytes, nstreams, resident=resident)
     # two warm-up passes: resident plans, then graphs of the multi-pass
     # requests (each runs again on the same buffers in every sweep point)
     for _ in range(2):
@@ -444,3 +446,203 @@ def compare(count=400, rates=(2000.0,), seed=11, n_max=2 ** 20, batch_max=512,
              "max_elems_per_request": max_elems, "mix_vs_alone_max_abs_diff": worst,
              "distinct_plans": len(cache.group) + len(cache.single)}
     return {"sweep": sweep, "notes": notes}
+
+
+# ----------------------------------------------------- configuration 5, full
+class _Ring:
+    """Output space for requests in flight: a ring over one device buffer.
+    A request gets the next free span (wrapping to the start); spans are
+    released when their request completes."""
+
+    def __init__(self, nbytes: int):
+        import torch
+        self.buf = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+        self.size = nbytes
+        self.head = 0
+        self.live = {}  # rid -> (start, end)
+
+    def alloc(self, nbytes: int, rid: int):
+        nbytes = (nbytes + 255) // 256 * 256
+        if nbytes > self.size:
+            raise ValueError("request larger than the output ring")
+        for start in (self.head, 0):
+            if start + nbytes > self.size:
+                continue
+            if all(e <= start or s >= start + nbytes for s, e in self.live.values()):
+                self.live[rid] = (start, start + nbytes)
+                self.head = start + nbytes
+                return start
+        return None
+
+    def view(self, start: int, r: "Request"):
+        import torch
+        dt = torch.complex64 if r.kind == "c64" else torch.complex128
+        es = ELEM[r.kind]
+        return self.buf[start:start + r.n * r.batch * es].view(dt).view(r.batch, r.n)
+
+    def free(self, rid: int):
+        self.live.pop(rid, None)
+
+
+class _Pools:
+    """Device-resident complex-normal input data, one pool per element type.
+    Request r reads n*batch consecutive values starting at an offset drawn
+    from its seed (inputs drawn from a pool rather than made per request, so
+    that 100k requests of up to 2^29 values fit on the device)."""
+
+    def __init__(self, elems: int, seed: int = 5):
+        import torch
+        self.elems = elems
+        self.pool = {}
+        for kind, rdt in (("c64", torch.float32), ("c128", torch.float64)):
+            g = torch.Generator(device="cuda").manual_seed(seed)
+            self.pool[kind] = torch.complex(
+                torch.randn(elems, generator=g, device="cuda", dtype=rdt),
+                torch.randn(elems, generator=g, device="cuda", dtype=rdt))
+
+    def input(self, r: "Request"):
+        m = r.n * r.batch
+        off = (r.seed % (self.elems - m + 1)) & ~1  # even: 16-byte aligned for ComplexF32
+        return self.pool[r.kind][off:off + m].view(r.batch, r.n)
+
+
+def _serve(srv: "Server", trace, pools: _Pools, ring: _Ring, t0_shift=0.0):
+    """Drive `srv` with the trace's arrivals; outputs in the ring (a request
+    is submitted once it has arrived and its output space is free).  Returns
+    per-request completion times (s, device clock) and the run's statistics."""
+    import torch
+    h = srv.h
+    n = len(trace)
+    arrivals = np.array([r.arrival for r in trace])
+    done = np.full(n, np.nan)
+    cap = 4096
+    tk = np.zeros(cap, dtype=np.int64)
+    tm = np.zeros(cap, dtype=np.float64)
+    cnt = ctypes.c_int64()
+    ticket_of = {}
+    tkt = ctypes.c_int64()
+    i64 = ctypes.POINTER(ctypes.c_int64)
+    st0 = srv.stats()
+    torch.cuda.synchronize()
+    _check(_lib.lib.fb_server_reset_clock(h))
+    t0 = time.perf_counter()
+    nxt, ndone, failed = 0, 0, 0
+    while ndone < n:
+        now = time.perf_counter() - t0
+        while nxt < n and arrivals[nxt] <= now:
+            r = trace[nxt]
+            start = ring.alloc(r.n * r.batch * ELEM[r.kind], nxt)
+            if start is None:
+                break  # output space frees as requests complete
+            x = pools.input(r)
+            y = ring.view(start, r)
+            _check(_lib.lib.fb_server_submit(h, r.n, Server.KIND[r.kind], r.dir, r.batch,
+                                             ctypes.c_void_p(x.data_ptr()),
+                                             ctypes.c_void_p(y.data_ptr()), ctypes.byref(tkt)))
+            ticket_of[tkt.value] = nxt
+            nxt += 1
+        _check(_lib.lib.fb_server_poll(h, cap, tk.ctypes.data_as(i64),
+                                       tm.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                       ctypes.byref(cnt)))
+        for j in range(cnt.value):
+            k = ticket_of.pop(int(tk[j]))
+            done[k] = tm[j] * 1e-3 if tm[j] >= 0 else np.nan
+            failed += tm[j] < 0
+            ring.free(k)
+        ndone += cnt.value
+        if cnt.value == 0 and nxt < n and ndone == nxt:
+            dt = arrivals[nxt] - (time.perf_counter() - t0)
+            if dt > 2e-4:
+                time.sleep(min(dt - 1e-4, 0.0005))
+    wall = time.perf_counter() - t0
+    st1 = srv.stats()
+    for r, d in zip(trace, done):
+        r.done = float(d)
+    out = _stats([r for r in trace if not math.isnan(r.done)], wall,
+                 "serial" if st1[1] and srv.serial else "continuous_batching")
+    out.update({"failed": int(failed), "launches": st1[1] - st0[1],
+                "descriptor_launches": st1[2] - st0[2],
+                "resident_kernel_requests": st1[9] - st0[9],
+                "graph_launches": st1[6] - st0[6], "plans_made": st1[11] - st0[11],
+                "plans_released": st1[12] - st0[12], "max_admitted_GB": st1[4] / 1e9})
+    return out
+
+
+def _schedule_class(n: int, kind: str) -> str:
+    lmax = 16384 if kind == "c64" else 8192
+    if _is_prime(n) and n >= 73:
+        return "bluestein"
+    return "one_pass" if n <= lmax else "multi_pass"
+
+
+def compare_config5(count=100000, seed=11, budget_bytes=100e9, nstreams=4,
+                    prefix=10000, prefix_rates=(1000.0, 3000.0), sample=240,
+                    pool_elems=1 << 29, ring_bytes=48 << 30, reference=None):
+    """Configuration 5 at its stated scale: `count` requests (length
+    log-uniform 64..2^20 in the class mix, batch 1..512, 80 % ComplexF32,
+    forward/backward 50/50), a 100 GB admission budget, served by the
+    continuous-batching server and by the same server in serial mode (one
+    request at a time, one plan launch each: the one-launch-per-request
+    path).  Both start cold (plans made on first use, least recently used
+    released), read inputs from a device pool and write into an output ring.
+
+    The full trace runs with every request queued at t0 (saturation); the
+    Poisson rate sweep runs on its first `prefix` requests.  Accuracy (when a
+    `reference(x, dir)` -- rows of x transformed in FP64 -- is given): a
+    stratified sample of `sample` requests (every schedule class and type)
+    is served again and its first transform compared with the reference."""
+    import torch
+    base = make_trace(count, 1.0, seed)
+    pools = _Pools(pool_elems)
+    ring = _Ring(ring_bytes)
+    result = {"requests": count, "budget_GB": budget_bytes / 1e9, "sweep": []}
+    runs = [("all_at_t0", 0.0, base)] + [(r, r, base[:prefix]) for r in prefix_rates]
+    for label, rate, tr in runs:
+        point = {"rate_req_s": label, "requests": len(tr)}
+        for name, serial in (("batched", False), ("one_launch_per_request", True)):
+            srv = Server(budget_bytes, nstreams, serial=serial)
+            reqs = [dataclasses.replace(r, arrival=(r.arrival / rate if rate > 0 else 0.0))
+                    for r in tr]
+            point[name] = _serve(srv, reqs, pools, ring)
+            del srv
+            torch.cuda.synchronize()
+        point["throughput_ratio"] = (point["batched"]["throughput_req_s"] /
+                                     point["one_launch_per_request"]["throughput_req_s"])
+        result["sweep"].append(point)
+    if reference is None:
+        return result
+    # accuracy on a stratified sample, served alone by the batched server
+    strata = collections.defaultdict(list)
+    for r in base:
+        strata[(_schedule_class(r.n, r.kind), r.kind)].append(r)
+    per = max(1, sample // max(1, len(strata)))
+    picked = [r for v in strata.values() for r in v[:per]]
+    srv = Server(budget_bytes, nstreams)
+    errs = collections.defaultdict(list)
+    import concurrent.futures as cf
+    with cf.ThreadPoolExecutor(max_workers=8) as ex:
+        jobs = []
+        for r in picked:
+            # the request's first transform, served alone into its own buffer
+            xin = pools.input(r)[0]
+            out = torch.empty(r.n, dtype=xin.dtype, device="cuda")
+            tkt = ctypes.c_int64()
+            _check(_lib.lib.fb_server_submit(srv.h, r.n, Server.KIND[r.kind], r.dir, 1,
+                                             ctypes.c_void_p(xin.data_ptr()),
+                                             ctypes.c_void_p(out.data_ptr()), ctypes.byref(tkt)))
+            _check(_lib.lib.fb_server_wait(srv.h))
+            x = xin.cpu().numpy().astype(np.complex128)
+            jobs.append((r, out.cpu().numpy(), ex.submit(reference, x[None, :], r.dir)))
+        for r, y, fut in jobs:
+            ref = fut.result()[0]
+            e = float(np.linalg.norm(y - ref) / np.linalg.norm(ref))
+            errs[(_schedule_class(r.n, r.kind), r.kind)].append(e)
+    del srv
+    acc = {}
+    for (cls, kind), v in sorted(errs.items()):
+        acc[f"{kind}/{cls}"] = {"requests": len(v), "max_rel_l2": max(v),
+                                "median_rel_l2": float(np.median(v))}
+    result["accuracy_vs_fp64_oracle"] = acc
+    result["max_rel_l2"] = {k: max(max(v) for (c, kk), v in errs.items() if kk == k)
+                            for k in ("c64", "c128") if any(kk == k for (_, kk) in errs)}
+    return result

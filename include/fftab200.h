@@ -3,8 +3,8 @@
  *
  * FFTA.jl is pure Julia; its entry points are AbstractFFTs methods.  Each
  * function below names the FFTA method it replaces (file:line inside the
- * FFTA.jl repository).  A Julia binding calls these with `ccall` (see
- * INTEGRATION.md); the Python package ffta_b200 calls them with ctypes.
+ * FFTA.jl repository).  The Julia package julia/FFTAB200 calls these with
+ * `ccall`; the Python package ffta_b200 calls them with ctypes.
  *
  * Conventions
  *  - Complex data are interleaved (re, im) pairs: ComplexF32 = 2 x float,
@@ -181,8 +181,16 @@ int fb_execute_grouped(fb_plan plan, int64_t count, const void* const* ins, void
  * of lines of the queued requests with the specialised stage programs.  Its
  * waits are bounded; a request whose descriptor does not arrive in time
  * completes with done_ms = -1 in fb_server_poll.  FB_SERVER_NO_PERSISTENT
- * sends those requests to the descriptor launches as well. */
-enum { FB_SERVER_NO_GRAPHS = 1u, FB_SERVER_NO_PERSISTENT = 2u };
+ * sends those requests to the descriptor launches as well.
+ * Multi-pass and large requests run plans kept per (length, type,
+ * direction, batch rounded up to a power of two, at least 512) on the
+ * request's own batch (fb_execute_batch); the least recently used idle plans
+ * are released while the plans' device bytes exceed a quarter of the budget.
+ * FB_SERVER_SERIAL makes the server the plain path it is compared with: one
+ * request at a time, each its own plan launch, the next one dispatched only
+ * after the previous one completed (no packing, no resident kernel, no
+ * graphs, the same plan cache). */
+enum { FB_SERVER_NO_GRAPHS = 1u, FB_SERVER_NO_PERSISTENT = 2u, FB_SERVER_SERIAL = 4u };
 typedef struct fb_server_s* fb_server;
 int fb_server_create(fb_server* srv, double budget_bytes, int nstreams, uint32_t flags);
 /* Queue `batch` contiguous transforms of length n (device pointers; the
@@ -215,10 +223,10 @@ int fb_server_cancel(fb_server srv, int64_t ticket);
 int fb_server_drop_next_descriptor(fb_server srv);
 /* Dispatch and wait until every submitted request has completed. */
 int fb_server_wait(fb_server srv);
-/* out[0..10]: requests, launches, descriptor launches, max queue depth, max
+/* out[0..12]: requests, launches, descriptor launches, max queue depth, max
  * admitted bytes, resident plans, graph launches, graph captures, cancelled
- * requests, requests served by the resident kernel, requests it gave up on
- * (the first `nout` of them). */
+ * requests, requests served by the resident kernel, requests it gave up on,
+ * plans made, plans released (the first `nout` of them). */
 int fb_server_stats(fb_server srv, int64_t* out, int nout);
 /* Restart the clock of fb_server_poll's completion times (waits until the
  * server's first stream is idle). */
