@@ -619,10 +619,10 @@ static bool tma_geometry(const fb_plan_s* P, const Pass& p, const LineArgs& a, T
   const size_t flat = (size_t)L * G * es;
   const size_t padded = (size_t)G * tile_pitch(lpad_for(L), G, es) * es;
   const size_t buf = (std::max(flat, padded) + 1023) / 1024 * 1024;
-  int nbuf = (int)std::min<size_t>(3, (110 * 1024) / buf);
-  if (nbuf < 2) nbuf = (int)std::min<size_t>(3, (220 * 1024) / buf);
-  if (getenv("FB_TMA_NBUF")) nbuf = std::min<int>(atoi(getenv("FB_TMA_NBUF")), (int)((220 * 1024) / buf));  // EXPERIMENT
-  if (nbuf < (getenv("FB_TMA_NBUF") ? 1 : 2)) return false;  // EXPERIMENT
+  // two tiles per block: one computing, one landing (measured: a third
+  // buffer costs more in resident blocks than it gains)
+  const int nbuf = 2;
+  if (nbuf * buf > 220 * 1024) return false;
   g->nbox = nbox;
   g->boxr = boxr;
   g->units = es / 8;
@@ -632,40 +632,40 @@ static bool tma_geometry(const fb_plan_s* P, const Pass& p, const LineArgs& a, T
   return true;
 }
 
-// Switch a lean tile pass to tensor-copy loads where it qualifies, with as
-// many lines per tile as give 128-byte rows (64 at least) within the block's
-// thread limit.
+// FB_FLAG_TMA: switch a lean tile pass to tensor-copy loads where it
+// qualifies, with the lines per tile that leave the most warps resident per
+// SM (two tile buffers per block; ties: the wider rows).  Opt-in: on the
+// four-step and strided-axis passes measured here the thread-loaded tile
+// kernel, with two blocks of 512 threads per SM, was faster.
 static void plan_tma(const fb_plan_s* P, Pass& p) {
-  if ((P->flags & FB_FLAG_NO_TMA) || !p.staged) return;
+  if (!(P->flags & FB_FLAG_TMA) || !p.staged) return;
   const int es = elem_bytes(P->dtype);
-  const int pol = getenv("FB_TMA_POLICY") ? atoi(getenv("FB_TMA_POLICY")) : 1;  // EXPERIMENT
-  if (pol == 0) return;  // EXPERIMENT
   int bestG = 0;
-  if (pol == 2) {  // EXPERIMENT: most resident warps per SM
-    double bw = 0;
-    for (int G = 128 / es; G * es >= 32; G /= 2) {
-      TmaGeom g;
-      LineArgs ag = p.a;
-      ag.G = G;
-      if (!tma_geometry(P, p, ag, &g)) continue;
-      const int thr = G * p.staged->T;
-      const int bs = std::min(std::min((int)((227 * 1024) / (g.nbuf * g.buf_bytes + 256)), 2048 / thr), 65536 / (thr * 64));
-      const double w = (double)bs * thr / 32 + G * 1e-3;
-      if (w > bw) { bw = w; bestG = G; }
-    }
-  }
+  double bw = 0;
   for (int G = 128 / es; G * es >= 32; G /= 2) {
     TmaGeom g;
-    if (bestG && G != bestG) continue;  // EXPERIMENT
     LineArgs ag = p.a;
     ag.G = G;
     if (!tma_geometry(P, p, ag, &g)) continue;
-    p.tma = 1;
-    p.tg = g;
-    p.a.G = G;
-    p.what += "<tma G=" + std::to_string(G) + " bufs=" + std::to_string(g.nbuf) + ">";
-    return;
+    const int thr = G * p.staged->T;
+    const int blocks = std::min(std::min((int)((227 * 1024) / (g.nbuf * g.buf_bytes + 256)),
+                                         2048 / thr),
+                                65536 / (thr * 64));
+    const double w = (double)blocks * thr / 32 + G * 1e-3;
+    if (w > bw) {
+      bw = w;
+      bestG = G;
+    }
   }
+  if (!bestG) return;
+  TmaGeom g;
+  LineArgs ag = p.a;
+  ag.G = bestG;
+  tma_geometry(P, p, ag, &g);
+  p.tma = 1;
+  p.tg = g;
+  p.a.G = bestG;
+  p.what += "<tma G=" + std::to_string(bestG) + " bufs=" + std::to_string(g.nbuf) + ">";
 }
 
 // CUtensorMap of a tensor-copy pass over the input `in` (4-D: lines in
@@ -1364,7 +1364,10 @@ static Axis plan_axis(fb_plan_s* P, int64_t n, int64_t is, int64_t os, std::vect
       // as the first pass (the strided columns)
       c *= 1.0 + 1e-9 * std::fabs(std::log((double)a) - std::log((double)b));
       if ((a & (a - 1)) == 0 && (b & (b - 1)) != 0) c *= 1.0 - 1e-6;
-      if (getenv("FB_FOUR_N1") && a == atoll(getenv("FB_FOUR_N1"))) c = 0;  // EXPERIMENT
+      // few neighbouring columns per transform (a short second factor) keep
+      // the first pass's tiles narrow: 27648 = 27 x 1024 measured 0.141 ms
+      // against 0.161 ms for 1024 x 27 (C32, 606 columns)
+      if (is == 1 && b < 128 && a > b) c *= 1.25;
       if (c < best) {
         best = c;
         bN1 = a;
@@ -2695,7 +2698,9 @@ int fb_server_create(fb_server* srv, double budget_bytes, int nstreams, uint32_t
     cuda_check(cudaEventSynchronize(S->start), "event sync");
     if (!(flags & (FB_SERVER_NO_PERSISTENT | FB_SERVER_SERIAL))) {
       PQueue* q = nullptr;
-      cuda_check(pq_create(&q, getenv("FB_PQ_IDLE_US") ? 1000ull * atoi(getenv("FB_PQ_IDLE_US")) : 100000ull), "persistent queue");  // EXPERIMENT
+      // the resident kernel ends after 100 us without work, so that it does
+      // not hold SMs that the plan launches of other requests need
+      cuda_check(pq_create(&q, 100000ull), "persistent queue");
       S->pq.reset(q);
       cuda_check(cudaHostAlloc((void**)&S->clk_host, sizeof(int64_t), cudaHostAllocMapped),
                  "clock");
@@ -2730,7 +2735,15 @@ int fb_server_submit(fb_server srv, int64_t n, int dtype, int dir, int64_t batch
     // a plan stream; small ones are packed into descriptor launches
     const bool packed = srv_single_pass(T) && n * batch < kPackedMaxElems;
     const SrvShape* shape = packed ? srv_shape(srv, T, dtype) : nullptr;
-    if (!shape) bytes += (double)plan_scratch_bytes(srv_multi(srv, n, dtype, dir, batch));
+    if (!shape || srv->serial) {
+      // the scratch this batch uses in its plan: one host-loop step's share
+      // of the plan's scratch per transform, at most the whole of it
+      const fb_plan_s* M = srv_multi(srv, n, dtype, dir, batch);
+      int64_t steps = 1;
+      for (auto& o : M->axes[0].outer) steps *= o.n;
+      const double per = (double)plan_scratch_bytes(M) / (double)(M->dims[1] / steps);
+      bytes += std::min((double)plan_scratch_bytes(M), per * (double)batch);
+    }
     // a request that could never be admitted is refused now, not queued for good
     if (bytes > srv->budget) refuse();
     SrvReq r{srv->next_ticket++, n, batch, dtype, dir, in, out, bytes, shape, srv->drop_next};

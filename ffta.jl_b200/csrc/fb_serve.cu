@@ -458,7 +458,10 @@ cudaError_t pq_create(PQueue** out, uint64_t idle_ns) {
   a.progs = (const PProg*)(d + off_prog);
   a.idle_ns = idle_ns;
   a.desc_wait_ns = 2000000;  // 2 ms
-  q->nblocks = std::min(per_sm, getenv("FB_PQ_BPS") ? atoi(getenv("FB_PQ_BPS")) : 1) * nsm;  // EXPERIMENT
+  // one block per SM: the rest of each SM stays free for the descriptor and
+  // plan launches of other requests (two per SM measured 13-15x against
+  // 18-19x for one, on the small-request trace)
+  q->nblocks = nsm;
   *out = q;
   return cudaSuccess;
 }

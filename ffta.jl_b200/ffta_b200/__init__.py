@@ -328,7 +328,7 @@ FB_FLAG_GENERIC_ONLY = 1  # include/fftab200.h: generic kernels only (for tests)
 FB_FLAG_SAME_SCHEDULE_STRIDED = 2  # strided axes bit-identical to contiguous ones
 FB_FLAG_STREAM = 4  # persistent bulk-copy kernel for contiguous lines (bit-identical)
 FB_FLAG_TENSOR_STAGE = 8  # C32: first radix-16 stage on the tensor cores (split BF16)
-FB_FLAG_NO_TMA = 16  # strided passes load thread by thread, not by tensor copies
+FB_FLAG_TMA = 16  # strided passes load tiles by tensor copies (opt-in; bit-identical)
 FB_FLAG_TUNE_RADIX = 32  # autotune also chooses the radix program (results not bitwise equal)
 FB_SERVER_NO_GRAPHS = 1  # fb_server_create: no CUDA-graph replay of recurring multi-pass requests
 FB_SERVER_NO_PERSISTENT = 2  # fb_server_create: no resident kernel; small requests in descriptor launches

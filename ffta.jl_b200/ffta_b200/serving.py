@@ -454,9 +454,9 @@ class _Ring:
     A request gets the next free span (wrapping to the start); spans are
     released when their request completes."""
 
-    def __init__(self, nbytes: int):
+    def __init__(self, nbytes: int, device="cuda"):
         import torch
-        self.buf = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+        self.buf = torch.empty(nbytes, dtype=torch.uint8, device=device)
         self.size = nbytes
         self.head = 0
         self.live = {}  # rid -> (start, end)

@@ -64,9 +64,11 @@ enum { FB_DEFAULT_BLUESTEIN_CUTOFF = 73 }; /* src/callgraph.jl:44 */
  *   of the FP32 butterflies.  Error stays at the FP32 path's level; results
  *   are not bit-identical to the default path.  No FFTA counterpart (FFTA
  *   computes in the element type only).
- * FB_FLAG_NO_TMA: load the tiles of strided passes (four-step columns,
- *   strided axes) thread by thread instead of with tensor copies into shared
- *   memory (bit-identical results; the flag exists so tests can check that).
+ * FB_FLAG_TMA: load the tiles of strided passes (four-step columns, strided
+ *   axes) with tensor copies (cp.async.bulk.tensor) into shared memory, two
+ *   tiles per persistent block, instead of thread by thread (bit-identical
+ *   results).  Opt-in: on B200 the thread-loaded kernel measured faster for
+ *   the four-step and 2-D column passes (more warps resident per SM).
  * FB_FLAG_TUNE_RADIX: let fb_plan_autotune also choose the radix program
  *   (the order and sizes of the butterfly stages) of each one-pass length of
  *   the plan among alternatives -- 16/8/4/2 groupings of the factor 2^a,
@@ -80,7 +82,7 @@ enum {
   FB_FLAG_SAME_SCHEDULE_STRIDED = 2u,
   FB_FLAG_STREAM = 4u,
   FB_FLAG_TENSOR_STAGE = 8u,
-  FB_FLAG_NO_TMA = 16u,
+  FB_FLAG_TMA = 16u,
   FB_FLAG_TUNE_RADIX = 32u
 };
 

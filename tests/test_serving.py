@@ -200,3 +200,22 @@ def test_resident_kernel_gives_up_on_a_lost_descriptor():
             assert err <= 4 * 2.0 ** -23 * 10, err
     finally:
         _lib.lib.fb_server_destroy(h)
+
+
+def test_output_ring_reuses_freed_space():
+    """The configuration-5 driver's output ring (host logic): spans never
+    overlap a live one, the ring wraps, and space frees on completion."""
+    ring = serving._Ring(4096, device="cpu")
+    a = ring.alloc(1500, 1)
+    b = ring.alloc(1500, 2)
+    assert (a, b) == (0, 1536)
+    assert ring.alloc(1500, 3) is None  # 3072 + 1536 > 4096 and [0, 1536) is live
+    ring.free(1)
+    c = ring.alloc(1500, 3)  # wraps to the start
+    assert c == 0
+    spans = sorted(ring.live.values())
+    assert all(e1 <= s2 for (s1, e1), (s2, e2) in zip(spans, spans[1:]))
+    with pytest.raises(ValueError):
+        ring.alloc(5000, 4)
+    r = serving.Request(0, 16, "c64", -1, 2, 0, 0.0)
+    assert ring.view(c, r).shape == (2, 16)

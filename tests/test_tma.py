@@ -1,11 +1,11 @@
 """Strided passes fed by tensor copies (cp.async.bulk.tensor into shared memory).
 
-The four-step column passes and strided axes whose lines are neighbours in
-memory (FFTA's composite transform, src/algos.jl:51-118, and the strided
-lines of fft_along_dim!, src/plan.jl:327-348) load whole tiles of G lines
-with tensor copies, several tiles ahead, instead of thread by thread.  Only
-the way data reaches shared memory changes, so results must equal the
-thread-loaded kernels (FB_FLAG_NO_TMA) bit for bit and the FP64 oracle within
+With FB_FLAG_TMA the four-step column passes and strided axes whose lines
+are neighbours in memory (FFTA's composite transform, src/algos.jl:51-118,
+and the strided lines of fft_along_dim!, src/plan.jl:327-348) load whole
+tiles of G lines with tensor copies, a tile ahead, instead of thread by
+thread.  Only the way data reaches shared memory changes, so results must
+equal the default thread-loaded kernels bit for bit and the FP64 oracle within
 4 eps log2 N.
 """
 import ctypes
@@ -55,8 +55,8 @@ def test_tensor_copies_equal_thread_loads(dims, region, kind):
     dt = torch.complex64 if kind == "c64" else torch.complex128
     x = _colmajor(dims, dt, sum(dims))
     for planner in (F.plan_fft, F.plan_bfft):
-        p = planner(x, region)
-        q = planner(x, region, _flags=F.FB_FLAG_NO_TMA)
+        p = planner(x, region, _flags=F.FB_FLAG_TMA)
+        q = planner(x, region)
         dp, dq = p.describe(x), q.describe(x)
         assert "<tma" in dp, dp
         assert "<tma" not in dq, dq
@@ -80,6 +80,8 @@ def test_unaligned_input_falls_back():
     y = torch.empty_like(x)  # same strides, aligned
     y.copy_(x)
     assert (x.data_ptr() % 16) != 0 and (y.data_ptr() % 16) == 0
-    p = F.plan_fft(x, 1)
+    p = F.plan_fft(x, 1, _flags=F.FB_FLAG_TMA)
+    assert "<tma" in p.describe(y)
     assert torch.equal(p * x, p * y)
+    assert torch.equal(p * x, F.plan_fft(x, 1) * x)
     assert _flag_clear()
