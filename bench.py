@@ -435,6 +435,41 @@ def main():
             precision[plabel] = row
             del xr, xj, yj
 
+    # real transforms: rfft of Float32 N=4096 x 16384 (FFTA's half-length
+    # algorithm, one kernel); bytes charged: the real input (4 N) and the
+    # n/2+1 complex outputs (8 (N/2+1)) per transform
+    real_out = {}
+    if not args.no_extra and rank == 0 and not args.workload:
+        for rlabel, rn, rb in (("f32_rfft_n4096_b16384", 4096, 16384),
+                               ("f32_rfft_n2048_b4096", 2048, 4096)):
+            gen = torch.Generator(device=dev).manual_seed(6)
+            xr = torch.randn(rb, rn, device=dev, generator=gen)
+            pr = F.plan_rfft(xr.T, 1)
+            yr = pr * xr.T
+            for _ in range(3):
+                yr = pr * xr.T
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(10):
+                yr = pr * xr.T
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1) / 10
+            rbytes = rb * (4.0 * rn + 8.0 * (rn // 2 + 1))
+            gbs = rbytes / (t * 1e-3) / 1e9
+            import oracle
+            cols = [0, rb // 2, rb - 1]
+            ref = oracle.fft_batched(xr[cols].cpu().numpy().astype(np.complex128), -1,
+                                     nthreads=os.cpu_count() or 1)[:, : rn // 2 + 1]
+            got = yr.T[cols].cpu().numpy()
+            real_out[rlabel] = {
+                "ms": t, "GB/s": gbs, "frac_of_hbm": gbs / peaks()[0],
+                "frac_of_spec_8tbs": gbs / SPEC_HBM_GBS,
+                "GFLOP/s": flops(rn, rb) / 2 / (t * 1e-3) / 1e9,
+                "rel_l2_vs_fp64_oracle": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
+                "schedule": pr.describe((rn, rb))}
+            del xr, yr, pr
+
     serving_out = None
     if rank == 0 and world == 1 and not args.no_serving and not args.workload:
         from ffta_b200 import serving as S
@@ -505,6 +540,7 @@ def main():
             "extra": extra,
             "serving": serving_out,
             "config4_precision": precision or None,
+            "real_transforms": real_out or None,
         }
         print(json.dumps(line))
     if world > 1:

@@ -2276,6 +2276,8 @@ struct fb_server_s {
 
 namespace fb {
 
+static bool srv_single_pass(const fb_plan_s* P);
+
 static fb_plan_s* srv_template(fb_server_s* S, int64_t n, int dtype, int dir) {
   auto key = std::make_tuple(n, dtype, dir);
   auto it = S->templ.find(key);
@@ -2286,12 +2288,19 @@ static fb_plan_s* srv_template(fb_server_s* S, int64_t n, int dtype, int dir) {
   std::vector<int> reg{0};
   fb_plan_s* P = create_plan(dtype, dir, 2, dims, st, st, reg, FB_DEFAULT_BLUESTEIN_CUTOFF,
                              FB_FLAG_GENERIC_ONLY);
+  if (!srv_single_pass(P)) {
+    // multi-pass lengths run their bucket plans; only the verdict is kept
+    // (tens of thousands of distinct lengths would otherwise hold their
+    // tables and scratch for good)
+    delete P;
+    P = nullptr;
+  }
   S->templ[key].reset(P);
   return P;
 }
 
 static bool srv_single_pass(const fb_plan_s* P) {
-  return P->axes.size() == 1 && P->axes[0].passes.size() == 1 && P->axes[0].outer.empty() &&
+  return P && P->axes.size() == 1 && P->axes[0].passes.size() == 1 && P->axes[0].outer.empty() &&
          P->axes[0].passes[0].a.ld.mode == 0 && P->axes[0].passes[0].a.st.mode == 0;
 }
 
@@ -2303,6 +2312,7 @@ static int64_t srv_bucket(int64_t batch) {
 }
 static size_t plan_scratch_bytes(const fb_plan_s* P);
 static void srv_release_plan(fb_server_s* S, const fb_plan_s* P);
+static void srv_trim_multi(fb_server_s* S, size_t cap);
 
 static fb_plan_s* srv_multi(fb_server_s* S, int64_t n, int dtype, int dir, int64_t batch) {
   auto key = std::make_tuple(n, dtype, dir, srv_bucket(batch));
@@ -2311,8 +2321,32 @@ static fb_plan_s* srv_multi(fb_server_s* S, int64_t n, int dtype, int dir, int64
     it->second.used = ++S->multi_clock;
     return it->second.P.get();
   }
-  // over the cap: release idle plans, least recently used first
-  while (S->multi_bytes > S->multi_cap && !S->multi.empty()) {
+  srv_trim_multi(S, S->multi_cap);
+  int64_t dims[2] = {n, srv_bucket(batch)}, st[2] = {1, n};
+  std::vector<int> reg{0};
+  fb_plan_s* P = nullptr;
+  try {
+    P = create_plan(dtype, dir, 2, dims, st, st, reg, FB_DEFAULT_BLUESTEIN_CUTOFF, 0);
+  } catch (const FbError& e) {
+    if (e.code != FB_ERR_OUT_OF_MEMORY) throw;
+    // device memory is short (other users of the device): release every
+    // idle plan and try once more
+    srv_trim_multi(S, 0);
+    P = create_plan(dtype, dir, 2, dims, st, st, reg, FB_DEFAULT_BLUESTEIN_CUTOFF, 0);
+  }
+  fb_server_s::MultiPlan& m = S->multi[key];
+  m.P.reset(P);
+  m.used = ++S->multi_clock;
+  m.bytes = P->table_bytes + plan_scratch_bytes(P);
+  S->multi_bytes += m.bytes;
+  S->st_plans_made += 1;
+  return P;
+}
+
+// Release idle multi-pass plans, least recently used first, while their
+// device bytes exceed `cap`.
+static void srv_trim_multi(fb_server_s* S, size_t cap) {
+  while (S->multi_bytes > cap && !S->multi.empty()) {
     auto lru = S->multi.end();
     for (auto m = S->multi.begin(); m != S->multi.end(); ++m) {
       if (m->second.ev && cudaEventQuery(m->second.ev) == cudaErrorNotReady) {
@@ -2328,16 +2362,6 @@ static fb_plan_s* srv_multi(fb_server_s* S, int64_t n, int dtype, int dir, int64
     S->multi.erase(lru);
     S->st_plans_released += 1;
   }
-  int64_t dims[2] = {n, srv_bucket(batch)}, st[2] = {1, n};
-  std::vector<int> reg{0};
-  fb_plan_s* P = create_plan(dtype, dir, 2, dims, st, st, reg, FB_DEFAULT_BLUESTEIN_CUTOFF, 0);
-  fb_server_s::MultiPlan& m = S->multi[key];
-  m.P.reset(P);
-  m.used = ++S->multi_clock;
-  m.bytes = P->table_bytes + plan_scratch_bytes(P);
-  S->multi_bytes += m.bytes;
-  S->st_plans_made += 1;
-  return P;
 }
 
 static size_t plan_scratch_bytes(const fb_plan_s* P) {

@@ -30,6 +30,7 @@ transforms, not data generation.
 """
 from __future__ import annotations
 
+import bisect
 import collections
 import ctypes
 import dataclasses
@@ -459,7 +460,9 @@ class _Ring:
         self.buf = torch.empty(nbytes, dtype=torch.uint8, device=device)
         self.size = nbytes
         self.head = 0
-        self.live = {}  # rid -> (start, end)
+        self.live = {}  # rid -> start
+        self.starts = []  # starts of the live spans, ascending
+        self.end = {}  # start -> end
 
     def alloc(self, nbytes: int, rid: int):
         nbytes = (nbytes + 255) // 256 * 256
@@ -468,10 +471,16 @@ class _Ring:
         for start in (self.head, 0):
             if start + nbytes > self.size:
                 continue
-            if all(e <= start or s >= start + nbytes for s, e in self.live.values()):
-                self.live[rid] = (start, start + nbytes)
-                self.head = start + nbytes
-                return start
+            i = bisect.bisect_left(self.starts, start)
+            if i < len(self.starts) and self.starts[i] < start + nbytes:
+                continue  # a live span starts inside
+            if i > 0 and self.end[self.starts[i - 1]] > start:
+                continue  # the previous live span reaches into it
+            self.starts.insert(i, start)
+            self.end[start] = start + nbytes
+            self.live[rid] = start
+            self.head = start + nbytes
+            return start
         return None
 
     def view(self, start: int, r: "Request"):
@@ -481,7 +490,10 @@ class _Ring:
         return self.buf[start:start + r.n * r.batch * es].view(dt).view(r.batch, r.n)
 
     def free(self, rid: int):
-        self.live.pop(rid, None)
+        start = self.live.pop(rid, None)
+        if start is not None:
+            del self.starts[bisect.bisect_left(self.starts, start)]
+            del self.end[start]
 
 
 class _Pools:
@@ -494,11 +506,11 @@ class _Pools:
         import torch
         self.elems = elems
         self.pool = {}
-        for kind, rdt in (("c64", torch.float32), ("c128", torch.float64)):
+        for kind, cdt in (("c64", torch.complex64), ("c128", torch.complex128)):
             g = torch.Generator(device="cuda").manual_seed(seed)
-            self.pool[kind] = torch.complex(
-                torch.randn(elems, generator=g, device="cuda", dtype=rdt),
-                torch.randn(elems, generator=g, device="cuda", dtype=rdt))
+            z = torch.empty(elems, dtype=cdt, device="cuda")
+            torch.view_as_real(z).normal_(generator=g)  # no temporaries
+            self.pool[kind] = z
 
     def input(self, r: "Request"):
         m = r.n * r.batch

@@ -213,9 +213,36 @@ def test_output_ring_reuses_freed_space():
     ring.free(1)
     c = ring.alloc(1500, 3)  # wraps to the start
     assert c == 0
-    spans = sorted(ring.live.values())
+    spans = sorted((s0, ring.end[s0]) for s0 in ring.live.values())
     assert all(e1 <= s2 for (s1, e1), (s2, e2) in zip(spans, spans[1:]))
     with pytest.raises(ValueError):
         ring.alloc(5000, 4)
     r = serving.Request(0, 16, "c64", -1, 2, 0, 0.0)
     assert ring.view(c, r).shape == (2, 16)
+
+
+def test_output_ring_random_against_brute_force():
+    """Random allocations and out-of-order frees: the ring's answer equals a
+    brute-force scan over the live spans (first fit at the head, else at 0)."""
+    rng = np.random.default_rng(3)
+    size = 1 << 16
+    ring = serving._Ring(size, device="cpu")
+    live, head = {}, 0
+    for rid in range(3000):
+        if live and rng.random() < 0.45:
+            k = list(live)[rng.integers(len(live))]
+            ring.free(k)
+            live.pop(k)
+            continue
+        nb = int(rng.integers(1, 6000))
+        rb = (nb + 255) // 256 * 256
+        want = None
+        for st in (head, 0):
+            if st + rb <= size and all(e <= st or s0 >= st + rb for s0, e in live.values()):
+                want = st
+                break
+        got = ring.alloc(nb, rid)
+        assert got == want
+        if got is not None:
+            live[rid] = (got, got + rb)
+            head = got + rb

@@ -40,7 +40,7 @@ CASES = [
     ((2 ** 20, 4), 1, "c64"),
     ((2 ** 20, 2), 1, "c128"),
     ((2 ** 15, 8), 1, "c64"),
-    ((2 ** 14 * 3, 4), 1, "c64"),
+    ((512, 1536), 2, "c64"),
     ((1000, 1000), (1, 2), "c64"),
     ((1000, 1000), (1, 2), "c128"),
     ((512, 1024), 2, "c64"),
