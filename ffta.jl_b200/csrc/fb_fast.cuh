@@ -479,15 +479,21 @@ template <class RL, int T> __host__ __device__ constexpr int max_values() {
 // Threads per tile block: up to 512, or 1024 for ComplexF32 lines of 256
 // threads outside Bluestein (four lines per block, so that a block covers a
 // whole 32-byte sector of each row of a strided axis).
+// The Bluestein MID variant (two programs and a product per line) takes at
+// most 256 threads per block (or T) at up to 80 registers, three blocks per
+// SM: with 512-thread bounds it took 128 registers and a 2048-point line's
+// 128-thread blocks ran four per SM.
 template <typename R, int T, bool MID> struct TileThreads {
-  static constexpr int value = (sizeof(R) == 4 && T == 256 && !MID) ? 1024 : (T > 512 ? T : 512);
+  static constexpr int value = MID ? (T > 256 ? T : 256)
+                                   : ((sizeof(R) == 4 && T == 256) ? 1024 : (T > 512 ? T : 512));
 };
 template <typename R, class RL, int T, bool MID, bool PLAIN> struct TileBounds {
   static constexpr int min_blocks =
-      (TileThreads<R, T, MID>::value <= 512 && !MID && T <= 512 &&
-       max_values<RL, T>() <= (sizeof(R) == 4 ? 18 : 9))
-          ? 2
-          : 1;
+      MID ? (T <= 256 ? 3 : 1)
+          : ((TileThreads<R, T, MID>::value <= 512 && T <= 512 &&
+              max_values<RL, T>() <= (sizeof(R) == 4 ? 18 : 9))
+                 ? 2
+                 : 1);
 };
 // Whether a tile launch reserves shared memory for a staged twiddle slice:
 // only four-step passes whose slice follows the second batch level.

@@ -32,7 +32,8 @@ namespace fb {
        : nullptr,                                                              \
    FastEntry<FB_R, RList<__VA_ARGS__>, T>::has_real                            \
        ? &FastEntry<FB_R, RList<__VA_ARGS__>, T>::launch_real                  \
-       : nullptr}
+       : nullptr,                                                              \
+   TileThreads<FB_R, T, true>::value}
 
 static const FastFn kTable[] = {
 #include "fb_fast_table.inc"

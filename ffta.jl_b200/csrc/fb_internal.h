@@ -179,6 +179,8 @@ struct FastFn {
   // half-length real transform of lines of length 2L (dir -1: rfft, +1:
   // brfft); nullptr where the length has none
   cudaError_t (*launch_real)(int dir, const RealArgs&, cudaStream_t);
+  // threads per block of launch_tile in Bluestein (MID) passes (G * T at most)
+  int mid_threads;
 };
 
 // Bytes of one direction's B table of the tensor-core radix-16 stage.

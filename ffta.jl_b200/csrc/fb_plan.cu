@@ -570,6 +570,7 @@ static void use_tile(const fb_plan_s* P, Pass& p, const std::vector<int>& radice
     G = std::max(G, std::min(std::min(4, thr_cap), g80));
   }
   if (em && p.a.tw_on_load && p.a.plain_io && G >= 4) G /= 2;
+  if (p.a.mid) G = std::min(G, std::max(1, ff->mid_threads / T));
   const int64_t nl = std::max<int64_t>(1, p.a.nlines);
   while (G > 1 && G / 2 >= nl) G /= 2;
   // lines contiguous on load: at least about four blocks per SM when the
@@ -2951,7 +2952,8 @@ static std::vector<Shape> pass_shapes(const fb_plan_s* P, const Pass& p) {
       if (G <= cap && (G == G0 || G <= nl) && (size_t)G * p.fast->lpad * es <= smem_max)
         out.push_back({G, T, 0});
   } else if (p.staged) {
-    const int T = p.staged->T, cap = tile_thread_cap(p.staged);
+    const int T = p.staged->T;
+    const int cap = p.a.mid ? std::max(1, p.staged->mid_threads / T) : tile_thread_cap(p.staged);
     for (int G : gs)
       if (G <= cap && (G == G0 || G <= nl) &&
           (size_t)G * (tile_pitch((int)p.staged->lpad, G, es) * es + 32) <= smem_max)

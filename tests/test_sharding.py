@@ -56,6 +56,50 @@ def test_two_rank_gloo():
         assert got == [1.0] * 10  # every column owned by exactly one rank
 
 
+def _failing_worker(rank, world, port, q, mode):
+    import datetime
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    if mode == "never_joins" and rank == 1:
+        return  # the rank dies before it joins the group
+    try:
+        dist.init_process_group("gloo", rank=rank, world_size=world,
+                                timeout=datetime.timedelta(seconds=5))
+    except Exception as e:  # rendezvous gave up: the other rank never came
+        q.put((rank, "init", type(e).__name__))
+        return
+    if mode == "raises" and rank == 1:
+        dist.destroy_process_group()
+        raise SystemExit(3)  # fails between steps, with nothing in flight
+    try:
+        sharding.max_over_ranks(1.0)  # the next step's collective
+        q.put((rank, "ok", ""))
+    except Exception as e:
+        q.put((rank, "collective", type(e).__name__))
+
+
+@pytest.mark.parametrize("mode", ["raises", "never_joins"])
+def test_rank_failure_is_seen_by_the_other(mode):
+    """A rank that fails between steps (or never joins) makes the surviving
+    rank's next collective (or the rendezvous) end with an error within the
+    group's short timeout instead of hanging."""
+    import time
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29400 + os.getpid() % 150 + (50 if mode == "raises" else 0)
+    procs = [ctx.Process(target=_failing_worker, args=(r, 2, port, q, mode)) for r in range(2)]
+    t0 = time.time()
+    for p in procs:
+        p.start()
+    rank, where, err = q.get(timeout=90)
+    for p in procs:
+        p.join(timeout=60)
+    assert rank == 0 and where in ("init", "collective") and err, (rank, where, err)
+    assert time.time() - t0 < 90
+    assert procs[1].exitcode != 0 or mode == "never_joins"
+
+
 def test_no_group_is_identity():
     assert sharding.max_over_ranks(3.0) == 3.0
     assert sharding.whole_job_rate(10, 2.0) == 5.0
