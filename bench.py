@@ -59,6 +59,15 @@ EXTRA = [
     ("c32_2d_2187x2048", "c32", (2187, 2048), 1),
     ("c32_2d_1000x1000", "c32", (1000, 1000), 1),
 ]
+# Workloads timed only on request (--workload), for profiling captures of
+# kernels the configurations above do not reach: the generic line kernel (a
+# length without a specialised kernel), the half-length real kernel, and the
+# opt-in tensor-copy tile feed.  (label, kind, dims, batch, plan flags name)
+PROFILE_ONLY = [
+    ("c32_n7168_b4096", "c32", (7168,), 4096, None),
+    ("f32_rfft_n4096_b8192", "r32", (4096,), 8192, None),
+    ("c32_n1048576_b16_tma", "c32", (2 ** 20,), 16, "FB_FLAG_TMA"),
+]
 
 
 SPEC_HBM_GBS = 8000.0  # B200 HBM3e specification, GB/s
@@ -70,8 +79,9 @@ SPEC_HBM_GBS = 8000.0  # B200 HBM3e specification, GB/s
 # launch, so that the write-back of an earlier launch's output still held in
 # L2 is counted like the steady state of the timed loop.  Traffic grows with
 # the columns, so the bench scales it by its batch / 4096.
-HEADLINE_TRAFFIC = (4096, 134.27e6 + 84.74e6,
-                    "ncu dram__bytes_read.sum + dram__bytes_write.sum, batch-4096 launch")
+HEADLINE_TRAFFIC = (4096, 132.317952e6 + 132.321536e6,
+                    "ncu dram__bytes_read.sum + dram__bytes_write.sum, third of three "
+                    "back-to-back batch-4096 launches (--cache-control none)")
 
 
 def flops(n, b):
@@ -241,6 +251,51 @@ def maybe_launch(gpus, argv):
     return subprocess.run(["timeout", "-k", "60", "1800"] + launch_command(gpus, argv)).returncode
 
 
+def run_profile_case(case, args, dev):
+    """One PROFILE_ONLY workload: warm-up, then `steps` timed steps (CUDA
+    events), a rel-L2 spot check against the FP64 oracle, one JSON line."""
+    import torch
+    import ffta_b200 as F
+    import oracle
+    label, kind, dims, batch, flag = case
+    flags = getattr(F, flag) if flag else 0
+    n = dims[0]
+    g = torch.Generator(device=dev).manual_seed(7)
+    if kind == "r32":
+        x = torch.randn(batch, n, device=dev, generator=g)
+        p = F.plan_rfft(x.T, 1)
+        alg = batch * (4.0 * n + 8.0 * (n // 2 + 1))
+        fl = flops(n, batch) / 2
+    else:
+        x = torch.randn(batch, n, dtype=torch.complex64, device=dev, generator=g)
+        p = F.plan_fft(x.T, 1, _flags=flags)
+        alg = 2.0 * n * batch * 8
+        fl = flops(n, batch)
+    y = p * x.T
+    for _ in range(args.warmup):
+        y = p * x.T
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        y = p * x.T
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    cols = [0, batch - 1]
+    xc = x[cols].cpu().numpy().astype(np.complex128)
+    ref = oracle.fft_batched(xc, -1, nthreads=os.cpu_count() or 1)
+    if kind == "r32":
+        ref = ref[:, : n // 2 + 1]
+    got = y.T[cols].cpu().numpy()
+    print(json.dumps({"workload": label, "ms": ms, "GB/s": alg / (ms * 1e-3) / 1e9,
+                      "GFLOP/s": fl / (ms * 1e-3) / 1e9,
+                      "rel_l2_vs_fp64_oracle": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
+                      "schedule": p.describe((n, batch)) if kind == "r32" else p.describe(x.T)}))
+    return 0
+
+
 def main():
     global BATCH
     ap = argparse.ArgumentParser()
@@ -258,7 +313,8 @@ def main():
                          "stage (ComplexF32 programs that start with 16)")
     ap.add_argument("--workload", default=None,
                     help="time one of the `extra` configurations instead of the headline "
-                         "(for profiling captures): " + ", ".join(e[0] for e in EXTRA))
+                         "(for profiling captures): " +
+                         ", ".join(e[0] for e in EXTRA + PROFILE_ONLY))
     args = ap.parse_args()
     rc = maybe_launch(args.gpus, sys.argv[1:])
     if rc is not None:
@@ -293,6 +349,9 @@ def main():
     g.manual_seed(1234 + rank)
     label, kind, dims, batch = "headline", "c32", (N,), BATCH
     if args.workload:
+        prof = [e for e in PROFILE_ONLY if e[0] == args.workload]
+        if prof:
+            return run_profile_case(prof[0], args, dev)
         sel = [e for e in EXTRA if e[0] == args.workload]
         if not sel:
             raise SystemExit(f"unknown workload {args.workload}")

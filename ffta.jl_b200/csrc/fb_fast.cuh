@@ -145,6 +145,12 @@ template <typename R> struct TileIn {
 };
 // Store with, in order: the table `mul` (chirp), the twiddle w_N^(dir*l0*i)
 // (hi/lo root tables), the scale.
+// prefetch.global.L1: a hint that brings the line into L1 (no register is
+// written; the address is one the kernel reads later).
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 template <typename R> struct TileOut {
   cplx<R>* __restrict__ base;
   int64_t es;
@@ -174,6 +180,14 @@ template <typename R> struct TileOut {
     }
     if (scale != R(1)) v = cscale<R>(v, scale);
     store<R>(base + (int64_t)i * es, v, cs);
+  }
+  // Bring the per-element tables element i's store will read (chirp, full
+  // twiddle table) into L1 ahead of time; the same presence test as above.
+  __device__ __forceinline__ void prefetch(int i) const {
+    const int64_t vi = (int64_t)i * ves + voff;
+    if (!ok || vi >= vn) return;
+    if (mul) prefetch_l1(mul + vi);
+    if (tab) prefetch_l1(tab + (int64_t)i * tab_es + tab_off);
   }
 };
 
@@ -337,6 +351,31 @@ __device__ __forceinline__ void fast_prog(cplx<R>* buf, const In& in, const Out&
   fast_stage<R, DIR, RL, S, T, In, Out, TC && S == 0>(buf, in, out, tw, pcs, u, tcx);
   if constexpr (S + 1 < RL::n)
     fast_prog<R, DIR, RL, T, In, Out, S + 1, TC>(buf, in, out, tw, pcs, u, tcx);
+}
+
+// Prefetch the store-time tables of the elements thread u stores in the last
+// stage (the index pattern of fast_stage's last stage), so that their loads
+// overlap the first loads and the stages: in a launch of about one wave every
+// block reaches its stores at the same time, and the table loads there would
+// otherwise wait out the memory latency with nothing else to run.
+template <typename R, class RL, int T>
+__device__ __forceinline__ void prefetch_store_tables(const TileOut<R>& o, int u) {
+  if (!o.ok || !(o.mul || o.tab)) return;
+  constexpr int S = RL::n - 1;
+  constexpr int RAD = RL::r[S];
+  constexpr int Ns = ns_before<RL, S>();
+  constexpr int nb = prog_len<RL>() / RAD;
+  constexpr int UM = (nb + T - 1) / T;
+#pragma unroll
+  for (int q = 0; q < UM; ++q) {
+    const int j = u + q * T;
+    if (nb % T == 0 || j < nb) {
+      const int k = (Ns == 1) ? 0 : j % Ns;
+      const int base = (j - k) * RAD + k;
+#pragma unroll
+      for (int r = 0; r < RAD; ++r) o.prefetch(base + r * Ns);
+    }
+  }
 }
 
 // ------------------------------------------------------ direct kernel
@@ -581,9 +620,12 @@ __global__ void __launch_bounds__(TileThreads<R, T, MID>::value,
                          a.tw_N ? (const C*)a.tw_hi : nullptr, (const C*)a.tw_lo, a.tw_shift,
                          a.tw_dir, (R)a.scale, ok, tout, a.tw_es, lt * a.tw_ls,
                          a.st_stream != 0};
+    prefetch_store_tables<R, RL, T>(out, u);
     if constexpr (MID) {
-      fast_prog<R, -1, RL, T>(buf, in, SmemIO{}, tw, pcs, u);
       const C* __restrict__ mid = (const C*)a.mid;
+      if (ok)
+        for (int k = u; k < L; k += T) prefetch_l1(mid + l0 * a.mid_ls + (int64_t)k * a.mid_es);
+      fast_prog<R, -1, RL, T>(buf, in, SmemIO{}, tw, pcs, u);
       for (int k = u; k < L; k += T)
         buf[pidx<RL>(k)] = cmul<R>(buf[pidx<RL>(k)], __ldg(mid + l0 * a.mid_ls + (int64_t)k * a.mid_es));
       __syncthreads();

@@ -497,24 +497,27 @@ class _Ring:
 
 
 class _Pools:
-    """Device-resident complex-normal input data, one pool per element type.
-    Request r reads n*batch consecutive values starting at an offset drawn
-    from its seed (inputs drawn from a pool rather than made per request, so
-    that 100k requests of up to 2^29 values fit on the device)."""
+    """Device-resident complex-normal input data, one pool per element type,
+    each as long as the largest request of its type.  Request r reads
+    n*batch consecutive values starting at an offset drawn from its seed
+    (inputs drawn from a pool rather than made per request, so that 100k
+    requests of up to 2^29 values fit on the device)."""
 
-    def __init__(self, elems: int, seed: int = 5):
+    def __init__(self, elems, seed: int = 5):
         import torch
-        self.elems = elems
+        self.elems = dict(elems)  # kind -> values
         self.pool = {}
         for kind, cdt in (("c64", torch.complex64), ("c128", torch.complex128)):
+            if self.elems.get(kind, 0) <= 0:
+                continue
             g = torch.Generator(device="cuda").manual_seed(seed)
-            z = torch.empty(elems, dtype=cdt, device="cuda")
+            z = torch.empty(self.elems[kind], dtype=cdt, device="cuda")
             torch.view_as_real(z).normal_(generator=g)  # no temporaries
             self.pool[kind] = z
 
     def input(self, r: "Request"):
         m = r.n * r.batch
-        off = (r.seed % (self.elems - m + 1)) & ~1  # even: 16-byte aligned for ComplexF32
+        off = (r.seed % (self.elems[r.kind] - m + 1)) & ~1  # even: 16-byte aligned
         return self.pool[r.kind][off:off + m].view(r.batch, r.n)
 
 
@@ -605,7 +608,11 @@ def compare_config5(count=100000, seed=11, budget_bytes=100e9, nstreams=4,
     is served again and its first transform compared with the reference."""
     import torch
     base = make_trace(count, 1.0, seed)
-    pools = _Pools(pool_elems)
+    need = collections.defaultdict(int)
+    for r in base:
+        need[r.kind] = max(need[r.kind], r.n * r.batch)
+    # at least `pool_elems` values, so that small requests read many offsets
+    pools = _Pools({k: max(v, min(pool_elems, v * 64)) for k, v in need.items()})
     ring = _Ring(ring_bytes)
     result = {"requests": count, "budget_GB": budget_bytes / 1e9, "sweep": []}
     runs = [("all_at_t0", 0.0, base)] + [(r, r, base[:prefix]) for r in prefix_rates]
