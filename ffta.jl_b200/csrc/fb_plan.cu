@@ -63,19 +63,116 @@ static void cuda_check(cudaError_t e, const char* what) {
 }
 
 // ----------------------------------------------------------- device memory
+// A cache of device blocks for plans that a serving loop makes and releases
+// by the thousand: a released block goes back to a free list of its size
+// class instead of to cudaFree, which waits for the whole device (every plan
+// release would drain the GPU).  Blocks are reused only by plans made under
+// the same cache, and the server releases only plans whose work has
+// completed.  Beyond `cap` cached bytes the least recently freed blocks are
+// given back with cudaFree, many at a time.
+struct BlockCache {
+  std::mutex mu_;
+  std::map<size_t, std::vector<void*>> free_;
+  std::deque<std::pair<size_t, void*>> order_;  // frees, oldest first
+  size_t cached = 0, cap;
+  explicit BlockCache(size_t c) : cap(c) {}
+  static size_t round(size_t b) {
+    if (b <= 4096) return 4096;
+    if (b <= (size_t(2) << 20)) {
+      size_t r = 4096;
+      while (r < b) r *= 2;
+      return r;
+    }
+    return (b + (size_t(2) << 20) - 1) / (size_t(2) << 20) * (size_t(2) << 20);
+  }
+  void* alloc(size_t b) {
+    std::lock_guard<std::mutex> lk(mu_);
+    const size_t r = round(b);
+    auto it = free_.find(r);
+    if (it != free_.end() && !it->second.empty()) {
+      void* p = it->second.back();
+      it->second.pop_back();
+      cached -= r;
+      for (auto o = order_.begin(); o != order_.end(); ++o)
+        if (o->second == p) {
+          order_.erase(o);
+          break;
+        }
+      return p;
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, r);
+    if (e == cudaErrorMemoryAllocation && cached) {
+      cudaGetLastError();
+      trim_locked(0);  // give the cached blocks back and try once more
+      e = cudaMalloc(&p, r);
+    }
+    cuda_check(e, "cudaMalloc");
+    return p;
+  }
+  void release(void* p, size_t b) {
+    std::lock_guard<std::mutex> lk(mu_);
+    const size_t r = round(b);
+    free_[r].push_back(p);
+    order_.emplace_back(r, p);
+    cached += r;
+    if (cached > cap) trim_locked(cap / 2);
+  }
+  void trim(size_t to) {
+    std::lock_guard<std::mutex> lk(mu_);
+    trim_locked(to);
+  }
+  void trim_locked(size_t to) {
+    while (cached > to && !order_.empty()) {
+      auto [r, p] = order_.front();
+      order_.pop_front();
+      auto& v = free_[r];
+      for (size_t i = 0; i < v.size(); ++i)
+        if (v[i] == p) {
+          v.erase(v.begin() + (long)i);
+          break;
+        }
+      cudaFree(p);
+      cached -= r;
+    }
+  }
+  ~BlockCache() { trim(0); }
+};
+// The cache DevBufs made on this thread draw from (set by the server while it
+// makes a plan), or null for plain cudaMalloc / cudaFree.
+static thread_local BlockCache* g_block_cache = nullptr;
+struct BlockCacheScope {
+  BlockCache* saved;
+  explicit BlockCacheScope(BlockCache* c) : saved(g_block_cache) { g_block_cache = c; }
+  ~BlockCacheScope() { g_block_cache = saved; }
+};
+
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  BlockCache* cache = nullptr;  // where the block goes back to
   DevBuf() = default;
-  explicit DevBuf(size_t b) : bytes(b) {
-    if (b) cuda_check(cudaMalloc(&p, b), "cudaMalloc");
+  explicit DevBuf(size_t b) : bytes(b), cache(g_block_cache) {
+    if (!b) return;
+    if (cache)
+      p = cache->alloc(b);
+    else
+      cuda_check(cudaMalloc(&p, b), "cudaMalloc");
   }
   ~DevBuf() {
-    if (p) cudaFree(p);
+    if (!p) return;
+    if (cache)
+      cache->release(p, bytes);
+    else
+      cudaFree(p);
   }
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
 };
+
+// Internal plan flag (above the public FB_FLAG_* bits): make the plan without
+// scratch buffers; its owner binds them (fb_plan_s::ext_s0/1) before use.
+constexpr uint32_t kFlagNoScratch = 1u << 30;
 
 // Per-device odd-prime cos/sin tables used by the register DFTs.
 struct DeviceTables {
@@ -474,6 +571,11 @@ struct fb_plan_s {
   std::vector<std::unique_ptr<fb::DevBuf>> bufs;  // tables
   size_t scratch_elems = 0;
   std::unique_ptr<fb::DevBuf> scratch0, scratch1;
+  // plans made without scratch (kFlagNoScratch, the server's): the buffers
+  // their passes use, bound by the owner before each execution
+  bool need_s1 = false;
+  void* ext_s0 = nullptr;
+  void* ext_s1 = nullptr;
   // host-execution staging
   std::unique_ptr<fb::DevBuf> hin, hout;
   // grouped execution: device copy of the request descriptors
@@ -1459,11 +1561,14 @@ static fb_plan_s* create_plan(int dtype, int dir, int rank, const int64_t* dims,
     }
   }
   if (P->scratch_elems) {
-    P->scratch0.reset(new DevBuf(P->scratch_elems * elem_bytes(dtype)));
     bool need1 = false;
     for (auto& ax : P->axes)
       for (auto& p : ax.passes) need1 |= p.src == B_S1 || p.dst == B_S1;
-    if (need1) P->scratch1.reset(new DevBuf(P->scratch_elems * elem_bytes(dtype)));
+    P->need_s1 = need1;
+    if (!(flags & kFlagNoScratch)) {
+      P->scratch0.reset(new DevBuf(P->scratch_elems * elem_bytes(dtype)));
+      if (need1) P->scratch1.reset(new DevBuf(P->scratch_elems * elem_bytes(dtype)));
+    }
   }
   cuda_check(cudaStreamSynchronize(0), "plan tables");
   apply_tuning(P.get());
@@ -1493,6 +1598,10 @@ static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s
   int dev = 0;
   cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
   if (dev != P->device) fail(FB_ERR_ARGUMENT, "plan was created on another device");
+  if (P->scratch_elems && !(P->scratch0 ? P->scratch0->p : P->ext_s0))
+    fail(FB_ERR_ARGUMENT, "plan has no scratch buffer bound");
+  if (P->need_s1 && !(P->scratch1 ? P->scratch1->p : P->ext_s1))
+    fail(FB_ERR_ARGUMENT, "plan has no second scratch buffer bound");
   const int es = elem_bytes(P->dtype);
   for (size_t ai = 0; ai < P->axes.size(); ++ai) {
     Axis& ax = P->axes[ai];
@@ -1523,8 +1632,8 @@ static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s
           switch (id) {
             case B_IN: return (char*)in + off * es;
             case B_OUT: return (char*)out + off * es;
-            case B_S0: return P->scratch0->p;
-            default: return P->scratch1->p;
+            case B_S0: return P->scratch0 ? P->scratch0->p : P->ext_s0;
+            default: return P->scratch1 ? P->scratch1->p : P->ext_s1;
           }
         };
         // outer offsets: the source of a first pass is the user input (axis 0)
@@ -2187,6 +2296,14 @@ struct SrvSlot {
 }  // namespace fb
 
 struct fb_server_s {
+  // device blocks of the plans this server makes and releases (declared
+  // first: destroyed after every plan that holds one)
+  std::unique_ptr<fb::BlockCache> cache;
+  // scratch of the multi-pass plans, one pair of buffers per plan stream
+  struct Arena {
+    std::unique_ptr<fb::DevBuf> s0, s1;
+  };
+  std::vector<Arena> arena;
   int device = 0;
   double budget = 100e9;
   std::vector<cudaStream_t> streams;
@@ -2283,10 +2400,16 @@ static fb_plan_s* srv_template(fb_server_s* S, int64_t n, int dtype, int dir) {
   auto key = std::make_tuple(n, dtype, dir);
   auto it = S->templ.find(key);
   if (it != S->templ.end()) return it->second.get();
+  if (n > lmax_for(dtype)) {
+    // beyond the generic kernel's line: never one generic pass
+    S->templ[key].reset();
+    return nullptr;
+  }
   // two contiguous transforms: the batch level of the lines is level 0 with
   // stride n, which the descriptors rewrite per request
   int64_t dims[2] = {n, 2}, st[2] = {1, n};
   std::vector<int> reg{0};
+  BlockCacheScope scope(S->cache.get());
   fb_plan_s* P = create_plan(dtype, dir, 2, dims, st, st, reg, FB_DEFAULT_BLUESTEIN_CUTOFF,
                              FB_FLAG_GENERIC_ONLY);
   if (!srv_single_pass(P)) {
@@ -2306,6 +2429,22 @@ static bool srv_single_pass(const fb_plan_s* P) {
 }
 
 static const int64_t kSrvMinBucket = 512;
+// Bytes of each scratch buffer a plan stream shares among its plans: the L2
+// chunk the four-step and Bluestein schedules cut their batch into, so every
+// plan of the served lengths fits (larger needs get their own).
+static const size_t kSrvArenaBytes = kL2Chunk;
+// Bind the scratch of plan P (made without its own) to the buffers of plan
+// stream si.  Plans of one stream never run at once, so they share them.
+static void srv_bind_scratch(fb_server_s* S, fb_plan_s* P, int si) {
+  if (!P->scratch_elems || P->scratch0) return;
+  auto& ar = S->arena[si];
+  if (!ar.s0) {
+    ar.s0.reset(new DevBuf(kSrvArenaBytes));
+    ar.s1.reset(new DevBuf(kSrvArenaBytes));
+  }
+  P->ext_s0 = ar.s0->p;
+  P->ext_s1 = ar.s1->p;
+}
 static int64_t srv_bucket(int64_t batch) {
   int64_t b = kSrvMinBucket;
   while (b < batch) b *= 2;
@@ -2326,14 +2465,22 @@ static fb_plan_s* srv_multi(fb_server_s* S, int64_t n, int dtype, int dir, int64
   int64_t dims[2] = {n, srv_bucket(batch)}, st[2] = {1, n};
   std::vector<int> reg{0};
   fb_plan_s* P = nullptr;
+  BlockCacheScope scope(S->cache.get());
   try {
-    P = create_plan(dtype, dir, 2, dims, st, st, reg, FB_DEFAULT_BLUESTEIN_CUTOFF, 0);
+    P = create_plan(dtype, dir, 2, dims, st, st, reg, FB_DEFAULT_BLUESTEIN_CUTOFF, kFlagNoScratch);
   } catch (const FbError& e) {
     if (e.code != FB_ERR_OUT_OF_MEMORY) throw;
     // device memory is short (other users of the device): release every
     // idle plan and try once more
     srv_trim_multi(S, 0);
-    P = create_plan(dtype, dir, 2, dims, st, st, reg, FB_DEFAULT_BLUESTEIN_CUTOFF, 0);
+    S->cache->trim(0);
+    P = create_plan(dtype, dir, 2, dims, st, st, reg, FB_DEFAULT_BLUESTEIN_CUTOFF, kFlagNoScratch);
+  }
+  // scratch above a plan stream's shared buffers: the plan's own
+  const size_t need = P->scratch_elems * elem_bytes(dtype);
+  if (need > kSrvArenaBytes) {
+    P->scratch0.reset(new DevBuf(need));
+    if (P->need_s1) P->scratch1.reset(new DevBuf(need));
   }
   fb_server_s::MultiPlan& m = S->multi[key];
   m.P.reset(P);
@@ -2475,7 +2622,10 @@ static void srv_reap_resident(fb_server_s* S) {
     int64_t t = 0;
     int32_t st = 0;
     if (pq_poll(S->pq.get(), q.r, &t, &st)) {
-      S->done.push_back({q.ticket, st == kPqStatOk ? (double)(t - S->clk0_ns) * 1e-6 : -1.0});
+      // failed: -1 when the descriptor never arrived, -2 without a program
+      S->done.push_back({q.ticket, st == kPqStatOk
+                                       ? (double)(t - S->clk0_ns) * 1e-6
+                                       : (st == kPqStatTimeout ? -1.0 : -2.0)});
       if (st != kPqStatOk) S->st_failed += 1;
       S->admitted -= q.bytes;
     } else {
@@ -2592,6 +2742,7 @@ static void srv_dispatch(fb_server_s* S) {
                  .emplace(P, (int)(S->next_multi_stream++ % S->multi_streams.size()))
                  .first;
       cudaStream_t mst = S->multi_streams[ms->second];
+      srv_bind_scratch(S, P, ms->second);
       srv_run_plan(S, P, r.in, r.out, r.batch, mst);
       {
         fb_server_s::MultiPlan& m =
@@ -2696,7 +2847,8 @@ int fb_server_create(fb_server* srv, double budget_bytes, int nstreams, uint32_t
     S->budget = budget_bytes > 0 ? budget_bytes : 100e9;
     S->serial = (flags & FB_SERVER_SERIAL) != 0;
     S->graphs = !(flags & FB_SERVER_NO_GRAPHS) && !S->serial;
-    S->multi_cap = (size_t)std::max(S->budget / 4, 1e9);
+    S->multi_cap = (size_t)std::max(S->budget / 2, 1e9);
+    S->cache.reset(new BlockCache(size_t(4) << 30));
     const int ns = std::max(1, std::min(nstreams, 16));
     for (int i = 0; i < ns; ++i) {
       cudaStream_t st;
@@ -2708,6 +2860,7 @@ int fb_server_create(fb_server* srv, double budget_bytes, int nstreams, uint32_t
       cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
       S->multi_streams.push_back(st);
     }
+    S->arena.resize(S->multi_streams.size());
     // descriptor slots sized for the largest dispatch up front: growing one
     // later frees device memory (which synchronises the device) and
     // allocates pinned memory in the middle of serving

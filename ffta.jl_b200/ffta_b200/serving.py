@@ -541,7 +541,7 @@ def _serve(srv: "Server", trace, pools: _Pools, ring: _Ring, t0_shift=0.0):
     torch.cuda.synchronize()
     _check(_lib.lib.fb_server_reset_clock(h))
     t0 = time.perf_counter()
-    nxt, ndone, failed = 0, 0, 0
+    nxt, ndone, failed, failed_no_program = 0, 0, 0, 0
     while ndone < n:
         now = time.perf_counter() - t0
         while nxt < n and arrivals[nxt] <= now:
@@ -563,6 +563,7 @@ def _serve(srv: "Server", trace, pools: _Pools, ring: _Ring, t0_shift=0.0):
             k = ticket_of.pop(int(tk[j]))
             done[k] = tm[j] * 1e-3 if tm[j] >= 0 else np.nan
             failed += tm[j] < 0
+            failed_no_program += tm[j] == -2.0
             ring.free(k)
         ndone += cnt.value
         if cnt.value == 0 and nxt < n and ndone == nxt:
@@ -575,7 +576,8 @@ def _serve(srv: "Server", trace, pools: _Pools, ring: _Ring, t0_shift=0.0):
         r.done = float(d)
     out = _stats([r for r in trace if not math.isnan(r.done)], wall,
                  "serial" if st1[1] and srv.serial else "continuous_batching")
-    out.update({"failed": int(failed), "launches": st1[1] - st0[1],
+    out.update({"failed": int(failed), "failed_without_program": int(failed_no_program),
+                "launches": st1[1] - st0[1],
                 "descriptor_launches": st1[2] - st0[2],
                 "resident_kernel_requests": st1[9] - st0[9],
                 "graph_launches": st1[6] - st0[6], "plans_made": st1[11] - st0[11],

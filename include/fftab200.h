@@ -179,15 +179,19 @@ int fb_execute_grouped(fb_plan plan, int64_t count, const void* const* ins, void
  * Small requests of length 16..4096 (powers of two) go instead to one
  * resident kernel: the server appends a work descriptor per request to a
  * queue in mapped host memory, and the kernel -- launched when work arrives
- * and none is resident, ending after 2 ms without new work -- claims chunks
- * of lines of the queued requests with the specialised stage programs.  Its
- * waits are bounded; a request whose descriptor does not arrive in time
- * completes with done_ms = -1 in fb_server_poll.  FB_SERVER_NO_PERSISTENT
+ * and none is resident, ending after 100 us without new work -- claims
+ * chunks of lines of the queued requests with the specialised stage
+ * programs.  Its waits are bounded; a request whose descriptor does not
+ * arrive in time completes with done_ms = -1 in fb_server_poll (-2 when its
+ * program was missing).  FB_SERVER_NO_PERSISTENT
  * sends those requests to the descriptor launches as well.
  * Multi-pass and large requests run plans kept per (length, type,
  * direction, batch rounded up to a power of two, at least 512) on the
  * request's own batch (fb_execute_batch); the least recently used idle plans
- * are released while the plans' device bytes exceed a quarter of the budget.
+ * are released while the plans' device bytes (their tables) exceed half
+ * the budget.  The plans bound to one plan stream share that
+ * stream's scratch buffers, and the device blocks of released plans are
+ * kept for the next plans (cudaFree would wait for the whole device).
  * FB_SERVER_SERIAL makes the server the plain path it is compared with: one
  * request at a time, each its own plan launch, the next one dispatched only
  * after the previous one completed (no packing, no resident kernel, no
