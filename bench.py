@@ -308,6 +308,9 @@ def main():
     ap.add_argument("--batch", type=int, default=BATCH,
                     help="columns per GPU (smaller for profiling captures)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving comparison")
+    ap.add_argument("--serving-config5", action="store_true",
+                    help="also serve configuration 5 at its stated scale (100k requests, "
+                         "batch 1..512, lengths 64..2^20, 100 GB budget; several minutes)")
     ap.add_argument("--tensor-stage", action="store_true",
                     help="time the main workload with the split-BF16 tensor-core radix-16 "
                          "stage (ComplexF32 programs that start with 16)")
@@ -548,6 +551,17 @@ def main():
                                          sat["one_launch_per_request"]["p99_ms"]},
                 **res}
         serving_out["recurring_multipass_graphs"] = S.compare_graphs()
+        if args.serving_config5:
+            import oracle
+            c5 = S.compare_config5(count=100000, prefix=10000, prefix_rates=(1000.0,),
+                                   sample=160, reference=oracle.fft_batched)
+            sat = c5["sweep"][0]
+            serving_out["config5"] = {
+                "saturated_throughput_ratio": sat["throughput_ratio"],
+                "saturated_p50_p99_ms": {
+                    k: [sat[k]["p50_ms"], sat[k]["p99_ms"]]
+                    for k in ("batched", "one_launch_per_request")},
+                **c5}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
