@@ -866,38 +866,13 @@ static void execute_plan(fb_plan_s* P, const void* in, void* out, cudaStream_t s
 
 // Chirp spectrum FFT_M(b_ext), forward, computed in FP64 by a C64 plan and
 // rounded to the plan type, optionally scaled.
-// The C64 plans of the pads (few distinct lengths), kept per (device, M):
-// a serving loop makes thousands of Bluestein plans of different lengths
-// over the same pads.  The least recently used of more than kSubPlans is
-// released; the mutex also serialises their use (their scratch is shared).
-static const size_t kSubPlans = 16;
-static std::mutex g_sub_mu;
-static std::map<std::pair<int, int64_t>, std::pair<int64_t, std::unique_ptr<fb_plan_s>>> g_sub;
-static int64_t g_sub_clock = 0;
-
 static void* chirp_spectrum(fb_plan_s* P, int64_t N, int64_t M, double scale) {
   DevBuf bext((size_t)M * 16), spec((size_t)M * 16);
   cuda_check(gen_chirp(P->dtype, nullptr, nullptr, bext.p, N, M, P->dir, 0), "chirp");
-  std::lock_guard<std::mutex> lk(g_sub_mu);
-  auto& slot = g_sub[{P->device, M}];
-  if (!slot.second) {
-    if (g_sub.size() > kSubPlans) {
-      auto lru = g_sub.end();
-      for (auto it = g_sub.begin(); it != g_sub.end(); ++it)
-        if (it->second.second && (lru == g_sub.end() || it->second.first < lru->second.first))
-          lru = it;
-      if (lru != g_sub.end()) g_sub.erase(lru);
-    }
-    // plain device memory: the plan outlives any server's block cache
-    BlockCacheScope plain(nullptr);
-    std::vector<int> reg{0};
-    int64_t d[1] = {M}, st[1] = {1};
-    g_sub[{P->device, M}].second.reset(
-        create_plan(FB_C64, FB_FORWARD, 1, d, st, st, reg, 1 << 30));
-  }
-  auto& sp = g_sub[{P->device, M}];
-  sp.first = ++g_sub_clock;
-  execute_plan(sp.second.get(), bext.p, spec.p, 0);
+  std::vector<int> reg{0};
+  int64_t d[1] = {M}, st[1] = {1};
+  std::unique_ptr<fb_plan_s> sub(create_plan(FB_C64, FB_FORWARD, 1, d, st, st, reg, 1 << 30));
+  execute_plan(sub.get(), bext.p, spec.p, 0);
   void* mid = alloc_table(P, (size_t)M * elem_bytes(P->dtype));
   cuda_check(convert_c64(P->dtype, mid, spec.p, M, scale, 0), "chirp spectrum");
   cuda_check(cudaStreamSynchronize(0), "chirp spectrum");
@@ -1159,8 +1134,6 @@ static Axis plan_direct_axis(fb_plan_s* P, int64_t n, LineX& x, int64_t is, int6
 // scratch (N * chunk elements, at most kL2Chunk bytes) stays in L2 between
 // pass 1 and pass 2; the chunks run one after the other (host loop).
 static const size_t kL2Chunk = 64u << 20;
-// Least pad elements per Bluestein chunk (see plan_blue3_axis).
-static const int64_t kBlueChunkElems = int64_t(1) << 24;
 
 static Axis plan_four_axis(fb_plan_s* P, int64_t N, int64_t N1, int64_t N2, LineX& x1, LineX& x2,
                            int64_t is, int64_t os, const std::vector<BDim>& bd, int src, int dst) {
@@ -1315,16 +1288,13 @@ static Axis plan_blue3_axis(fb_plan_s* P, int64_t N, int64_t is, int64_t os,
   std::vector<BDim> inner;
   split_levels(bd, 2, &inner, &ax.outer);
   if (!inner.empty()) {
-    // as in the four-step: the batch in chunks, one after the other, so the
-    // scratch stays bounded.  A chunk may hold up to kBlueChunkElems pad
-    // elements: a Bluestein pass over fewer runs as
-    // one short wave of blocks whose time is their latency (a 2^21 pad in
-    // 64 MB chunks of 4 lines served config-5 requests at 0.17 TB/s); above
-    // that, as many lines as fit kL2Chunk, so the scratch stays in L2.
+    // as in the four-step: the batch in chunks whose scratch (M * chunk
+    // elements per buffer) is at most kL2Chunk, one after the other, so the
+    // scratch stays bounded (and in L2 between the passes); chunks of up to
+    // 2^24 pad elements measured no faster on configuration-5 requests
     const int64_t B0c = inner[0].n;
-    const int64_t per = std::max<int64_t>(
-        std::max<int64_t>(1, (int64_t)(kL2Chunk / ((size_t)M * elem_bytes(P->dtype)))),
-        kBlueChunkElems / M);
+    const int64_t per =
+        std::max<int64_t>(1, (int64_t)(kL2Chunk / ((size_t)M * elem_bytes(P->dtype))));
     if (B0c > per) {
       int64_t chunk = 1;
       for (int64_t c = per; c >= 1; --c)
@@ -2460,11 +2430,10 @@ static bool srv_single_pass(const fb_plan_s* P) {
 }
 
 static const int64_t kSrvMinBucket = 512;
-// Bytes of each scratch buffer a plan stream shares among its plans: the
-// largest chunk the four-step (kL2Chunk) and Bluestein (kBlueChunkElems
-// ComplexF64 pad elements) schedules cut their batch into, so every plan of
-// the served lengths fits (larger needs get their own).
-static const size_t kSrvArenaBytes = std::max<size_t>(kL2Chunk, (size_t)kBlueChunkElems * 16);
+// Bytes of each scratch buffer a plan stream shares among its plans: the L2
+// chunk the four-step and Bluestein schedules cut their batch into, so every
+// plan of the served lengths fits (larger needs get their own).
+static const size_t kSrvArenaBytes = kL2Chunk;
 // Bind the scratch of plan P (made without its own) to the buffers of plan
 // stream si.  Plans of one stream never run at once, so they share them.
 static void srv_bind_scratch(fb_server_s* S, fb_plan_s* P, int si) {
