@@ -498,6 +498,9 @@ static bool make_line(int64_t n, int64_t cutoff, int dtype, LineX* x) {
 // length's kernels come to copy bandwidth: powers of two from 256 (radix-16
 // programs) 1.0, lines shorter than 16 2.0, others 1.25 -- measured on the
 // four-step splits of 27648: 1024 x 27 in 0.182 ms, 144 x 192 in 0.226 ms.
+// Cost factor of a four-step factor that has no compiled kernel.
+static const double kGenericPassCost = 3.0;
+
 static double line_cost(const LineX& x, bool weighted = false) {
   const double L = x.L;
   const double c = L * (std::log2(std::max(2.0, L)) + 4.0);
@@ -1463,7 +1466,15 @@ static Axis plan_axis(fb_plan_s* P, int64_t n, int64_t is, int64_t os, std::vect
       if (!make_line(a, P->cutoff, P->dtype, &xa) || !make_line(b, P->cutoff, P->dtype, &xb)) continue;
       if (prefer_split && (xa.kind != 0 || xb.kind != 0)) continue;
       const bool weighted = (n & (n - 1)) != 0;
-      double c = line_cost(xa, weighted) * (double)b + line_cost(xb, weighted) * (double)a;
+      // a factor without a compiled kernel runs on the generic one, about
+      // three times slower per element (measured on configuration-5
+      // lengths: 200-600 GB/s against 1300-1900 GB/s); decided without
+      // FB_FLAG_GENERIC_ONLY so that such plans keep the same split
+      const auto gen = [&](const LineX& x) {
+        return x.kind == 0 && !find_fast(P->dtype, x.L, x.radices) ? kGenericPassCost : 1.0;
+      };
+      double c = line_cost(xa, weighted) * gen(xa) * (double)b +
+                 line_cost(xb, weighted) * gen(xb) * (double)a;
       // prefer balanced direct splits on ties, and the power-of-two factor
       // as the first pass (the strided columns)
       c *= 1.0 + 1e-9 * std::fabs(std::log((double)a) - std::log((double)b));
