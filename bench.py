@@ -308,9 +308,9 @@ def main():
     ap.add_argument("--batch", type=int, default=BATCH,
                     help="columns per GPU (smaller for profiling captures)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving comparison")
-    ap.add_argument("--serving-config5", action="store_true",
-                    help="also serve configuration 5 at its stated scale (100k requests, "
-                         "batch 1..512, lengths 64..2^20, 100 GB budget; several minutes)")
+    ap.add_argument("--no-serving-config5", action="store_true",
+                    help="skip configuration 5 at its stated scale (100k requests, batch "
+                         "1..512, lengths 64..2^20, 100 GB budget; about five minutes)")
     ap.add_argument("--tensor-stage", action="store_true",
                     help="time the main workload with the split-BF16 tensor-core radix-16 "
                          "stage (ComplexF32 programs that start with 16)")
@@ -551,10 +551,12 @@ def main():
                                          sat["one_launch_per_request"]["p99_ms"]},
                 **res}
         serving_out["recurring_multipass_graphs"] = S.compare_graphs()
-        if args.serving_config5:
+        if not args.no_serving_config5:
             import oracle
-            c5 = S.compare_config5(count=100000, prefix=10000, prefix_rates=(1000.0,),
-                                   sample=160, reference=oracle.fft_batched)
+            print("bench: serving configuration 5 (100k requests, both paths)",
+                  file=sys.stderr, flush=True)
+            c5 = S.compare_config5(count=100000, prefix=10000, prefix_rates=(1000.0, 3000.0),
+                                   sample=240, reference=oracle.fft_batched)
             sat = c5["sweep"][0]
             serving_out["config5"] = {
                 "saturated_throughput_ratio": sat["throughput_ratio"],
