@@ -67,6 +67,30 @@ def test_one_launch_for_mixed_requests():
 
 
 @pytest.mark.gpu
+def test_multipass_plans_share_stream_scratch():
+    """Multi-pass requests of different schedules (four-step, three-pass
+    Bluestein, a four-step with a Bluestein factor) and both types, all on
+    one plan stream, so every plan uses that stream's shared scratch in turn;
+    each is served twice in the same mix (the second time by a cached plan
+    whose tables may come from the server's block cache).  Every result must
+    equal the same transform run alone through its own plan, bit for bit."""
+    import torch
+    import ffta_b200 as F
+    spec = [(20000, "c64", -1, 3), (100003, "c64", 1, 2), (3 * 2 ** 17, "c64", -1, 2),
+            (30030, "c128", 1, 3), (65537, "c64", -1, 2), (2 ** 8 * 4099, "c64", 1, 1),
+            (27648, "c128", -1, 2)]
+    spec = spec + spec
+    reqs = [serving.Request(i, n, k, d, b, i, 0.0) for i, (n, k, d, b) in enumerate(spec)]
+    xs = serving.make_inputs(reqs, "cuda")
+    ys = [torch.empty_like(x) for x in xs]
+    st = serving.Server(nstreams=1, graphs=False).run(reqs, xs, ys)
+    assert st["requests"] == len(reqs)
+    for r, x, y in zip(reqs, xs, ys):
+        f = F.fft if r.dir < 0 else F.bfft
+        assert torch.equal(y, f(x.T, 1).T), (r.n, r.kind, r.dir, r.batch)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("graphs", [True, False])
 def test_recurring_multipass_requests_replay_graphs(graphs):
     """Multi-pass requests (three-pass Bluestein, four-step) and large
