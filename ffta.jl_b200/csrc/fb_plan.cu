@@ -28,6 +28,7 @@
 #include <functional>
 #include <deque>
 #include <map>
+#include <set>
 #include <tuple>
 #include <memory>
 #include <mutex>
@@ -72,9 +73,10 @@ static void cuda_check(cudaError_t e, const char* what) {
 // given back with cudaFree, many at a time.
 struct BlockCache {
   std::mutex mu_;
-  std::map<size_t, std::vector<void*>> free_;
-  std::deque<std::pair<size_t, void*>> order_;  // frees, oldest first
-  size_t cached = 0, cap;
+  std::map<size_t, std::set<void*>> free_;      // cached blocks per size class
+  std::deque<std::pair<size_t, void*>> order_;  // frees, oldest first (may hold
+                                                // entries of blocks reused since)
+  size_t cached = 0, nblocks = 0, cap;
   explicit BlockCache(size_t c) : cap(c) {}
   static size_t round(size_t b) {
     if (b <= 4096) return 4096;
@@ -90,14 +92,10 @@ struct BlockCache {
     const size_t r = round(b);
     auto it = free_.find(r);
     if (it != free_.end() && !it->second.empty()) {
-      void* p = it->second.back();
-      it->second.pop_back();
+      void* p = *it->second.begin();
+      it->second.erase(it->second.begin());
       cached -= r;
-      for (auto o = order_.begin(); o != order_.end(); ++o)
-        if (o->second == p) {
-          order_.erase(o);
-          break;
-        }
+      nblocks -= 1;
       return p;
     }
     void* p = nullptr;
@@ -113,10 +111,20 @@ struct BlockCache {
   void release(void* p, size_t b) {
     std::lock_guard<std::mutex> lk(mu_);
     const size_t r = round(b);
-    free_[r].push_back(p);
+    free_[r].insert(p);
     order_.emplace_back(r, p);
     cached += r;
+    nblocks += 1;
     if (cached > cap) trim_locked(cap / 2);
+    if (order_.size() > 4 * nblocks + 1024) {
+      // drop the entries of blocks that were reused
+      std::deque<std::pair<size_t, void*>> keep;
+      for (auto& e : order_) {
+        auto f = free_.find(e.first);
+        if (f != free_.end() && f->second.count(e.second)) keep.push_back(e);
+      }
+      order_.swap(keep);
+    }
   }
   void trim(size_t to) {
     std::lock_guard<std::mutex> lk(mu_);
@@ -126,14 +134,11 @@ struct BlockCache {
     while (cached > to && !order_.empty()) {
       auto [r, p] = order_.front();
       order_.pop_front();
-      auto& v = free_[r];
-      for (size_t i = 0; i < v.size(); ++i)
-        if (v[i] == p) {
-          v.erase(v.begin() + (long)i);
-          break;
-        }
+      auto f = free_.find(r);
+      if (f == free_.end() || !f->second.erase(p)) continue;  // reused since
       cudaFree(p);
       cached -= r;
+      nblocks -= 1;
     }
   }
   ~BlockCache() { trim(0); }
