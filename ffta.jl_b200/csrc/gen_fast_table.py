@@ -4,7 +4,8 @@ Each entry's radix list is the planner's radix program for that length
 (fb_plan.cu radix_program: radix 16 with a trailing 8*4 / 4 / 8 / 2 for powers
 of two, radix 9 with a trailing 3 for powers of three, then 5s and odd primes)
 for the lengths below (powers of two and three, 2^a*3, 2^a*9, 5-smooth 5^c*2^a)
-and T = L / (largest radix) threads per line (at most 512; 1024 from 16384 up).
+and T = L / (largest radix) threads per line (at most 512; 1024 from 16384 up
+and where L / (largest radix) exceeds 512).
 Entries are spread over PARTS compilation units so they build in parallel.
 
 Run:  python gen_fast_table.py   (rewrites fb_fast_table.inc next to it)
@@ -68,9 +69,16 @@ def main():
     for L in lengths():
         rad = radix_program(L)
         T = L // max(rad)
-        if L == 16384:
+        if L == 16384 or (T > 512 and max(rad) == 16):
+            # more radix-16 butterflies per stage than 512 threads: one per
+            # thread on 1024 threads (16 values each, 64 registers, one block
+            # per SM) rather than two per thread on 512 (32 values, 128
+            # registers, one block of half the warps): the 9216-point
+            # Bluestein pad of 2^8 * 4099 x 4 went from 0.240 to 0.214 ms.
+            # Radix-8/9 programs (5000, 6561) measured within a few percent
+            # either way and keep 512.
             T = 1024
-        T = min(T, 1024 if L >= 16384 else 512)
+        T = min(T, 1024 if L >= 16384 or T == 1024 else 512)
         wide = L * 16 > 8192 * 16  # longer than the ComplexF64 line limit
         ents.append((L, T, rad, wide))
     for part in range(PARTS):
