@@ -251,6 +251,44 @@ def maybe_launch(gpus, argv):
     return subprocess.run(["timeout", "-k", "60", "1800"] + launch_command(gpus, argv)).returncode
 
 
+def reference_benchmark_sizes():
+    """The size categories of FFTA's own benchmark suite
+    (benchmark/common_defs.jl): odd powers of two 2^1..2^19, even powers
+    2^2..2^20, powers of three 3^1..3^9, the cumulative products of
+    3, 4, 5, 5, 7, 11, and the primes nearest to 20 log-spaced points between
+    2 and 20000 (duplicates dropped).  Returns {n: category}."""
+    def is_prime(v):
+        if v < 2:
+            return False
+        f = 2
+        while f * f <= v:
+            if v % f == 0:
+                return False
+            f += 1
+        return True
+    cats = {}
+    for i in range(1, 20, 2):
+        cats[2 ** i] = "odd_power_of_2"
+    for i in range(2, 21, 2):
+        cats[2 ** i] = "even_power_of_2"
+    for i in range(1, 10):
+        cats[3 ** i] = "power_of_3"
+    c = 1
+    for f in (3, 4, 5, 5, 7, 11):
+        c *= f
+        cats[c] = "composite"
+    primes = [v for v in range(2, 20001) if is_prime(v)]
+    chosen = []
+    for k in range(20):
+        target = np.exp(np.log(2.0) + (np.log(20000.0) - np.log(2.0)) * k / 19)
+        best = min(primes, key=lambda q: abs(q - target))
+        if best not in chosen:
+            chosen.append(best)
+    for q in chosen:
+        cats[q] = "prime"
+    return dict(sorted(cats.items()))
+
+
 def run_profile_case(case, args, dev):
     """One PROFILE_ONLY workload: warm-up, then `steps` timed steps (CUDA
     events), a rel-L2 spot check against the FP64 oracle, one JSON line."""
@@ -532,6 +570,62 @@ def main():
                 "schedule": pr.describe((rn, rb))}
             del xr, yr, pr
 
+    # FFTA's own benchmark (benchmark/bench_ffta.jl): one ComplexF64 fft and
+    # one Float64 rfft of each size category, median time per call; here per
+    # call through the Python mirror on device-resident data (CUDA events
+    # around each call, so the host's call overhead counts when it exceeds
+    # the kernel), with the oracle's single-threaded CPU time of the same
+    # complex transform beside it and rel-L2 against the FP64 oracle
+    sweep_out = []
+    if not args.no_extra and rank == 0 and not args.workload:
+        import oracle
+        gsw = torch.Generator(device=dev).manual_seed(9)
+        for n, cat in reference_benchmark_sizes().items():
+            xc = torch.randn(n, dtype=torch.complex128, device=dev, generator=gsw)
+            pc = F.plan_fft(xc, 1)
+            yc = pc * xc
+            ts = []
+            for it in range(23):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                F.mul_(yc, pc, xc)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                if it >= 3:
+                    ts.append(e0.elapsed_time(e1))
+            xh = xc.cpu().numpy()[None, :]
+            ref = oracle.fft_batched(xh, -1)[0]
+            rel = float(np.linalg.norm(yc.cpu().numpy() - ref) / np.linalg.norm(ref))
+            cpu_ts, t_end = [], time.perf_counter() + 0.2
+            while time.perf_counter() < t_end or not cpu_ts:
+                t0 = time.perf_counter()
+                oracle.fft_batched(xh, -1)
+                cpu_ts.append(time.perf_counter() - t0)
+            xr = torch.randn(n, dtype=torch.float64, device=dev, generator=gsw)
+            pr = F.plan_rfft(xr, 1)
+            yr = pr * xr
+            rts = []
+            for it in range(23):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                yr = pr * xr
+                e1.record(stream)
+                torch.cuda.synchronize()
+                if it >= 3:
+                    rts.append(e0.elapsed_time(e1))
+            rref = oracle.fft_batched(xr.cpu().numpy().astype(np.complex128)[None, :], -1)[0]
+            rref = rref[: n // 2 + 1]
+            rrel = float(np.linalg.norm(yr.cpu().numpy() - rref) / np.linalg.norm(rref))
+            ms = float(np.median(ts))
+            sweep_out.append({
+                "size": n, "category": cat,
+                "fft_c64_median_ms": ms, "fft_ns_per_element": ms * 1e6 / n,
+                "fft_rel_l2_vs_fp64_oracle": rel,
+                "cpu_oracle_1thread_median_ms": float(np.median(cpu_ts)) * 1e3,
+                "rfft_f64_median_ms": float(np.median(rts)),
+                "rfft_rel_l2_vs_fp64_oracle": rrel})
+            del xc, yc, pc, xr, yr, pr
+
     serving_out = None
     if rank == 0 and world == 1 and not args.no_serving and not args.workload:
         from ffta_b200 import serving as S
@@ -616,6 +710,7 @@ def main():
             "serving": serving_out,
             "config4_precision": precision or None,
             "real_transforms": real_out or None,
+            "reference_size_sweep": sweep_out or None,
         }
         print(json.dumps(line))
     if world > 1:
