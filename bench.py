@@ -525,10 +525,10 @@ def main():
                 e1.record(stream)
                 torch.cuda.synchronize()
                 t = e0.elapsed_time(e1) / 10
-                y = yj.cpu().numpy()
+                y4 = yj.cpu().numpy()
                 en = int(np.prod(pdims))
                 row[name] = {"ms": t, "GB/s": 2.0 * en * 8 / (t * 1e-3) / 1e9,
-                             "rel_l2_vs_fp64_oracle": float(np.linalg.norm(y - ref) /
+                             "rel_l2_vs_fp64_oracle": float(np.linalg.norm(y4 - ref) /
                                                             np.linalg.norm(ref)),
                              "tensor_core_passes": pp.describe(xj).count("<tc>"),
                              "schedule": pp.describe(xj)}
@@ -595,7 +595,7 @@ def main():
                     ts.append(e0.elapsed_time(e1))
             xh = xc.cpu().numpy()[None, :]
             ref = oracle.fft_batched(xh, -1)[0]
-            rel = float(np.linalg.norm(yc.cpu().numpy() - ref) / np.linalg.norm(ref))
+            frel = float(np.linalg.norm(yc.cpu().numpy() - ref) / np.linalg.norm(ref))
             cpu_ts, t_end = [], time.perf_counter() + 0.2
             while time.perf_counter() < t_end or not cpu_ts:
                 t0 = time.perf_counter()
@@ -616,11 +616,11 @@ def main():
             rref = oracle.fft_batched(xr.cpu().numpy().astype(np.complex128)[None, :], -1)[0]
             rref = rref[: n // 2 + 1]
             rrel = float(np.linalg.norm(yr.cpu().numpy() - rref) / np.linalg.norm(rref))
-            ms = float(np.median(ts))
+            fms = float(np.median(ts))
             sweep_out.append({
                 "size": n, "category": cat,
-                "fft_c64_median_ms": ms, "fft_ns_per_element": ms * 1e6 / n,
-                "fft_rel_l2_vs_fp64_oracle": rel,
+                "fft_c64_median_ms": fms, "fft_ns_per_element": fms * 1e6 / n,
+                "fft_rel_l2_vs_fp64_oracle": frel,
                 "cpu_oracle_1thread_median_ms": float(np.median(cpu_ts)) * 1e3,
                 "rfft_f64_median_ms": float(np.median(rts)),
                 "rfft_rel_l2_vs_fp64_oracle": rrel})
