@@ -196,24 +196,40 @@ template <typename R> struct TileOut {
 // line index is clamped to a valid line, so loads need no predicate.
 // `tab` is a generic pointer: the twiddle table in global memory, or the
 // line's slice of it staged in shared memory (then tab_es = 1, tab_off = 0).
-template <typename R> struct PlainIn {
+//
+// TW fixes at compile time what a functor multiplies by: kTwRuntime tests
+// `tab` and `tw_dir` at every element; kTwNone has no table; -1 / +1 always
+// apply the table, as w (forward) or conj(w) (backward).  PlainOut's SCALE =
+// false leaves out the scale (a scale of 1).  The four-step and 2-D passes
+// take the fixed forms, so their unrolled stages carry no per-element tests
+// of launch-wide values; the arithmetic is the same in every form.
+constexpr int kTwRuntime = 0, kTwNone = 2;
+template <typename R, int TW = kTwRuntime> struct PlainIn {
   const cplx<R>* __restrict__ base;
   int es;
   const cplx<R>* tab;  // twiddle on load (LineArgs::tw_on_load)
   int tab_es, tab_off, tw_dir;
+  __device__ __forceinline__ bool has_tab() const {
+    return TW == kTwRuntime ? tab != nullptr : TW != kTwNone;
+  }
+  __device__ __forceinline__ cplx<R> twm(cplx<R> v, cplx<R> w) const {
+    if constexpr (TW == -1)
+      return cmul<R>(v, w);
+    else if constexpr (TW == 1)
+      return cmulc<R>(v, w);
+    else
+      return tw_dir < 0 ? cmul<R>(v, w) : cmulc<R>(v, w);
+  }
   __device__ __forceinline__ cplx<R> raw(int i) const { return __ldcs(base + (int64_t)(i * es)); }
   __device__ __forceinline__ cplx<R> fin(int i, cplx<R> v) const {
-    if (tab) {
-      const cplx<R> w = tab[i * tab_es + tab_off];
-      v = tw_dir < 0 ? cmul<R>(v, w) : cmulc<R>(v, w);
-    }
+    if (has_tab()) v = twm(v, tab[i * tab_es + tab_off]);
     return v;
   }
   // The twiddles of butterfly j's inputs i = j + r*nb (tw_elem's product):
   // ceil(RAD/4) entries of its own plus the line's steps t(c*nb), c = 1..3.
   template <int RAD>
   __device__ __forceinline__ void fin_bfly(int j, int nb, cplx<R>* v) const {
-    if (!tab) return;
+    if (!has_tab()) return;
     if constexpr (RAD < 4) {
 #pragma unroll
       for (int r = 0; r < RAD; ++r) v[r] = fin(j + r * nb, v[r]);
@@ -228,7 +244,7 @@ template <typename R> struct PlainIn {
         for (int c = 0; c < 4; ++c) {
           if (a + c < RAD) {
             const cplx<R> w = c == 0 ? b : cmul<R>(b, s[c]);
-            v[a + c] = tw_dir < 0 ? cmul<R>(v[a + c], w) : cmulc<R>(v[a + c], w);
+            v[a + c] = twm(v[a + c], w);
           }
         }
       }
@@ -236,8 +252,8 @@ template <typename R> struct PlainIn {
   }
 };
 template <class In> struct InHasBfly : std::false_type {};
-template <typename R> struct InHasBfly<PlainIn<R>> : std::true_type {};
-template <typename R> struct PlainOut {
+template <typename R, int TW> struct InHasBfly<PlainIn<R, TW>> : std::true_type {};
+template <typename R, int TW = kTwRuntime, bool SCALE = true> struct PlainOut {
   cplx<R>* __restrict__ base;
   int es;
   const cplx<R>* tab;
@@ -246,11 +262,16 @@ template <typename R> struct PlainOut {
   bool ok;
   bool cs;
   __device__ __forceinline__ void operator()(int i, cplx<R> v) const {
-    if (tab) {
+    if (TW == kTwRuntime ? tab != nullptr : TW != kTwNone) {
       const cplx<R> w = tab[i * tab_es + tab_off];
-      v = tw_dir < 0 ? cmul<R>(v, w) : cmulc<R>(v, w);
+      if constexpr (TW == -1)
+        v = cmul<R>(v, w);
+      else if constexpr (TW == 1)
+        v = cmulc<R>(v, w);
+      else
+        v = tw_dir < 0 ? cmul<R>(v, w) : cmulc<R>(v, w);
     }
-    if (scale != R(1)) v = cscale<R>(v, scale);
+    if (SCALE && scale != R(1)) v = cscale<R>(v, scale);
     if (ok) store<R>(base + (int64_t)(i * es), v, cs);
   }
 };
@@ -604,13 +625,44 @@ __global__ void __launch_bounds__(TileThreads<R, T, MID>::value,
     const C* tout = a.tw_on_load ? nullptr : (const C*)a.tw_tab;
     const C* st = stage_twiddles<C>(a, lb + 3 * G, G, L, (C*)(lb + 4 * G), g + G * u, G * T);
     const int tes = st ? 1 : (int)a.tw_es, toff = st ? 0 : (int)(lt * a.tw_ls);
-    const PlainIn<R> in{ib, (int)a.ld.es, tin ? (st ? st : tin) : nullptr, tes, toff, a.tw_dir};
-    const PlainOut<R> out{ob, (int)a.st.es, tout ? (st ? st : tout) : nullptr, tes, toff,
-                          a.tw_dir, (R)a.scale, ok, a.st_stream != 0};
-    if (a.dir1 < 0)
-      fast_prog<R, -1, RL, T>(buf, in, out, tw, pcs, u);
-    else
-      fast_prog<R, 1, RL, T>(buf, in, out, tw, pcs, u);
+    const C* ti = tin ? (st ? st : tin) : nullptr;
+    const C* to = tout ? (st ? st : tout) : nullptr;
+    const int ies = (int)a.ld.es, oes = (int)a.st.es;
+    const bool cs = a.st_stream != 0;
+    // The lean passes of the four-step and 2-D schedules -- no twiddle, or a
+    // twiddle on the loads or on the stores in the transform's direction,
+    // and no scale -- run with those choices fixed at compile time; any other
+    // lean launch takes the run-time form.
+    const bool fixed = (R)a.scale == R(1) && !(ti && to) && (!(ti || to) || a.tw_dir == a.dir1);
+    if (fixed && !ti && !to) {
+      const PlainIn<R, kTwNone> in{ib, ies, nullptr, 0, 0, 0};
+      const PlainOut<R, kTwNone, false> out{ob, oes, nullptr, 0, 0, 0, R(1), ok, cs};
+      if (a.dir1 < 0)
+        fast_prog<R, -1, RL, T>(buf, in, out, tw, pcs, u);
+      else
+        fast_prog<R, 1, RL, T>(buf, in, out, tw, pcs, u);
+    } else if (fixed && ti) {
+      const PlainOut<R, kTwNone, false> out{ob, oes, nullptr, 0, 0, 0, R(1), ok, cs};
+      if (a.dir1 < 0)
+        fast_prog<R, -1, RL, T>(buf, PlainIn<R, -1>{ib, ies, ti, tes, toff, -1}, out, tw, pcs, u);
+      else
+        fast_prog<R, 1, RL, T>(buf, PlainIn<R, 1>{ib, ies, ti, tes, toff, 1}, out, tw, pcs, u);
+    } else if (fixed) {
+      const PlainIn<R, kTwNone> in{ib, ies, nullptr, 0, 0, 0};
+      if (a.dir1 < 0)
+        fast_prog<R, -1, RL, T>(buf, in, PlainOut<R, -1, false>{ob, oes, to, tes, toff, -1, R(1), ok, cs},
+                                tw, pcs, u);
+      else
+        fast_prog<R, 1, RL, T>(buf, in, PlainOut<R, 1, false>{ob, oes, to, tes, toff, 1, R(1), ok, cs},
+                               tw, pcs, u);
+    } else {
+      const PlainIn<R> in{ib, ies, ti, tes, toff, a.tw_dir};
+      const PlainOut<R> out{ob, oes, to, tes, toff, a.tw_dir, (R)a.scale, ok, cs};
+      if (a.dir1 < 0)
+        fast_prog<R, -1, RL, T>(buf, in, out, tw, pcs, u);
+      else
+        fast_prog<R, 1, RL, T>(buf, in, out, tw, pcs, u);
+    }
   } else {
     const C* tin = a.tw_on_load ? (const C*)a.tw_tab : nullptr;
     const C* tout = a.tw_on_load ? nullptr : (const C*)a.tw_tab;
