@@ -334,6 +334,67 @@ def run_profile_case(case, args, dev):
     return 0
 
 
+def run_size_sweep(dev, stream):
+    """FFTA's own benchmark (benchmark/bench_ffta.jl): one ComplexF64 fft and
+    one Float64 rfft of each size category, median time per call; here per
+    call through the Python mirror on device-resident data (CUDA events
+    around each call, so the host's call overhead counts when it exceeds the
+    kernel), with the oracle's single-threaded CPU time of the same complex
+    transform beside it and rel-L2 against the FP64 oracle."""
+    import oracle
+    import torch
+
+    import ffta_b200 as F
+    sweep_out = []
+    gsw = torch.Generator(device=dev).manual_seed(9)
+    for n, cat in reference_benchmark_sizes().items():
+        xc = torch.randn(n, dtype=torch.complex128, device=dev, generator=gsw)
+        pc = F.plan_fft(xc, 1)
+        yc = pc * xc
+        ts = []
+        for it in range(23):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            F.mul_(yc, pc, xc)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if it >= 3:
+                ts.append(e0.elapsed_time(e1))
+        xh = xc.cpu().numpy()[None, :]
+        ref = oracle.fft_batched(xh, -1)[0]
+        frel = float(np.linalg.norm(yc.cpu().numpy() - ref) / np.linalg.norm(ref))
+        cpu_ts, t_end = [], time.perf_counter() + 0.2
+        while time.perf_counter() < t_end or not cpu_ts:
+            t0 = time.perf_counter()
+            oracle.fft_batched(xh, -1)
+            cpu_ts.append(time.perf_counter() - t0)
+        xr = torch.randn(n, dtype=torch.float64, device=dev, generator=gsw)
+        pr = F.plan_rfft(xr, 1)
+        yr = pr * xr
+        rts = []
+        for it in range(23):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            yr = pr * xr
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if it >= 3:
+                rts.append(e0.elapsed_time(e1))
+        rref = oracle.fft_batched(xr.cpu().numpy().astype(np.complex128)[None, :], -1)[0]
+        rref = rref[: n // 2 + 1]
+        rrel = float(np.linalg.norm(yr.cpu().numpy() - rref) / np.linalg.norm(rref))
+        fms = float(np.median(ts))
+        sweep_out.append({
+            "size": n, "category": cat,
+            "fft_c64_median_ms": fms, "fft_ns_per_element": fms * 1e6 / n,
+            "fft_rel_l2_vs_fp64_oracle": frel,
+            "cpu_oracle_1thread_median_ms": float(np.median(cpu_ts)) * 1e3,
+            "rfft_f64_median_ms": float(np.median(rts)),
+            "rfft_rel_l2_vs_fp64_oracle": rrel})
+        del xc, yc, pc, xr, yr, pr
+    return sweep_out
+
+
 def main():
     global BATCH
     ap = argparse.ArgumentParser()
@@ -570,61 +631,9 @@ def main():
                 "schedule": pr.describe((rn, rb))}
             del xr, yr, pr
 
-    # FFTA's own benchmark (benchmark/bench_ffta.jl): one ComplexF64 fft and
-    # one Float64 rfft of each size category, median time per call; here per
-    # call through the Python mirror on device-resident data (CUDA events
-    # around each call, so the host's call overhead counts when it exceeds
-    # the kernel), with the oracle's single-threaded CPU time of the same
-    # complex transform beside it and rel-L2 against the FP64 oracle
     sweep_out = []
     if not args.no_extra and rank == 0 and not args.workload:
-        import oracle
-        gsw = torch.Generator(device=dev).manual_seed(9)
-        for n, cat in reference_benchmark_sizes().items():
-            xc = torch.randn(n, dtype=torch.complex128, device=dev, generator=gsw)
-            pc = F.plan_fft(xc, 1)
-            yc = pc * xc
-            ts = []
-            for it in range(23):
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                F.mul_(yc, pc, xc)
-                e1.record(stream)
-                torch.cuda.synchronize()
-                if it >= 3:
-                    ts.append(e0.elapsed_time(e1))
-            xh = xc.cpu().numpy()[None, :]
-            ref = oracle.fft_batched(xh, -1)[0]
-            frel = float(np.linalg.norm(yc.cpu().numpy() - ref) / np.linalg.norm(ref))
-            cpu_ts, t_end = [], time.perf_counter() + 0.2
-            while time.perf_counter() < t_end or not cpu_ts:
-                t0 = time.perf_counter()
-                oracle.fft_batched(xh, -1)
-                cpu_ts.append(time.perf_counter() - t0)
-            xr = torch.randn(n, dtype=torch.float64, device=dev, generator=gsw)
-            pr = F.plan_rfft(xr, 1)
-            yr = pr * xr
-            rts = []
-            for it in range(23):
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                yr = pr * xr
-                e1.record(stream)
-                torch.cuda.synchronize()
-                if it >= 3:
-                    rts.append(e0.elapsed_time(e1))
-            rref = oracle.fft_batched(xr.cpu().numpy().astype(np.complex128)[None, :], -1)[0]
-            rref = rref[: n // 2 + 1]
-            rrel = float(np.linalg.norm(yr.cpu().numpy() - rref) / np.linalg.norm(rref))
-            fms = float(np.median(ts))
-            sweep_out.append({
-                "size": n, "category": cat,
-                "fft_c64_median_ms": fms, "fft_ns_per_element": fms * 1e6 / n,
-                "fft_rel_l2_vs_fp64_oracle": frel,
-                "cpu_oracle_1thread_median_ms": float(np.median(cpu_ts)) * 1e3,
-                "rfft_f64_median_ms": float(np.median(rts)),
-                "rfft_rel_l2_vs_fp64_oracle": rrel})
-            del xc, yc, pc, xr, yr, pr
+        sweep_out = run_size_sweep(dev, stream)
 
     serving_out = None
     if rank == 0 and world == 1 and not args.no_serving and not args.workload:
