@@ -543,13 +543,20 @@ template <class RL, int T> __host__ __device__ constexpr int max_values() {
 // most 256 threads per block (or T) at up to 80 registers, three blocks per
 // SM: with 512-thread bounds it took 128 registers and a 2048-point line's
 // 128-thread blocks ran four per SM.
+// The ComplexF32 2048-point MID variant (T = 128) takes one line per block
+// at up to 72 registers, seven blocks per SM: the 1024 middle-pass blocks of
+// a 2^21-point Bluestein pad then fit one wave of 148 SMs (six blocks per SM
+// at 80 registers made it 1.15 waves).
+template <typename R, int T> struct MidOneLine {
+  static constexpr bool value = sizeof(R) == 4 && T == 128;
+};
 template <typename R, int T, bool MID> struct TileThreads {
-  static constexpr int value = MID ? (T > 256 ? T : 256)
+  static constexpr int value = MID ? (T > 256 ? T : (MidOneLine<R, T>::value ? T : 256))
                                    : ((sizeof(R) == 4 && T == 256) ? 1024 : (T > 512 ? T : 512));
 };
 template <typename R, class RL, int T, bool MID, bool PLAIN> struct TileBounds {
   static constexpr int min_blocks =
-      MID ? (T <= 256 ? 3 : 1)
+      MID ? (MidOneLine<R, T>::value ? 7 : (T <= 256 ? 3 : 1))
           : ((TileThreads<R, T, MID>::value <= 512 && T <= 512 &&
               max_values<RL, T>() <= (sizeof(R) == 4 ? 18 : 9))
                  ? 2
