@@ -2460,7 +2460,7 @@ static fb_plan_s* srv_template(fb_server_s* S, int64_t n, int dtype, int dir) {
   fb_plan_s* P = create_plan(dtype, dir, 2, dims, st, st, reg, FB_DEFAULT_BLUESTEIN_CUTOFF,
                              FB_FLAG_GENERIC_ONLY);
   if (!srv_single_pass(P)) {
-    // multi-pass lengths run their bucket plans; only the verdict is kept
+    // multi-pass lengths run their bucket plans; only the single-pass answer is kept
     // (tens of thousands of distinct lengths would otherwise hold their
     // tables and scratch for good)
     delete P;
