@@ -793,9 +793,9 @@ __global__ void __launch_bounds__(DirectBounds<R, T>::threads, DirectBounds<R, T
 // then every stage runs as in fast_tile_kernel, in the same buffer, and the
 // last stage stores to HBM from registers; the arithmetic is the same, so
 // results equal the other kernels' bit for bit.  Tensor maps cover this GPU's
-// own memory only and no copy is multicast.  Every wait is bounded: a block
-// that gives up sets kErrWaitTimeout, drains its copies in flight (at least
-// the default limit) and returns.
+// own memory only, and each copy lands in its own block's shared memory.
+// Every wait is bounded: a block that gives up sets kErrWaitTimeout, drains
+// its copies in flight (at least the default limit) and returns.
 
 // One box of a 4-D tensor map (x: lines in 8-byte units, y: elements of the
 // line, z/w: batch levels) into shared memory, completing on *bar.
